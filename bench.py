@@ -1,0 +1,420 @@
+"""Benchmark: photoelectric system-matrix entries per second on B200.
+
+Workload (``pe_large``): 64x64x32 voxels of 0.5 mm, two tungsten plates with
+400 seeded holes each, 4 layers of 40x40 crystals (6400 rows x 131072
+columns, 3.4 GB float32), 4x4x4 voxel sub-samples x 2x4x2 crystal sub-cells
+= 1024 rays per entry.  A step is one z-slab of 4 planes for every crystal
+(6400 x 16384 entries, the reference CLI's slab size); 8 steps cover the
+whole matrix.  Inputs are seeded synthetic tables (no public dataset exists
+for this path).
+
+``--impl ours`` (default) times the sm_100a kernel through the C ABI with the
+geometry resident on the device (``value``), then end to end through the
+public API with host tables in and the slab copied back to pinned host memory
+(``e2e``).  It also times the reference's own CUDA kernel on the same GPU on a
+bounded sample (``ref_cuda``) and the reference's code on the host cores
+(``cpu_baseline``).  ``--impl reference`` times the reference's CPU
+implementation (the reference kernel code compiled for the host, OpenMP over
+entries) on a bounded sample per step.
+
+Multi-GPU (torchrun): ranks take different slabs (weak scaling, no
+collective on the data path); the time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "gpu-spect-pet-sysmat_b200"))
+
+SLAB_Z = 4
+L2_FLUSH_BYTES = 256 << 20
+
+# FP32 operations per unit of work, counted from the tracer's source
+# (gpu-spect-pet-sysmat_b200/csrc/tracer.cuh, pe_kernel.cu): add/sub/mul/fma
+# and each div/sqrt/exp as 1.  Used for the roofline numerator.
+F_RAY = 64          # sub-cell point, distance, solid angle, self path, absorption, two exp
+F_BOX = 31          # chord_through, general case
+F_XF = 18           # crystal-frame transform of both ray ends
+F_CYL = 60          # chord_hole
+F_CONE = 26         # one candidate cone test
+F_IN = 31           # chord_to_end
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "of measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0}, "of fallback"
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def pe_workload(name: str):
+    from sysmat_b200 import configs
+    return configs.NAMED[name]()
+
+
+# ---------------------------------------------------------------------------
+# CPU side: the reference's own code on the host cores
+# ---------------------------------------------------------------------------
+
+def cpu_reference_rate(p, target_s: float, seed: int = 0, max_entries: int = 1 << 16):
+    """Entries/s of the reference kernel code on all host cores, on a seeded
+    random sample of entries grown until it takes >= target_s."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_py
+    kind = "f32"
+    if not oracle_py.ref_available("pe_f32"):
+        return None
+    rng = np.random.default_rng(seed)
+    n, spent, done = 64, 0.0, 0
+    while spent < target_s and done < max_entries:
+        rows = rng.integers(0, p.n_crystals, n)
+        vox = rng.integers(0, p.n_voxels, n)
+        t0 = time.perf_counter()
+        oracle_py.ref_pe_entries(p, rows, vox, kind)
+        spent += time.perf_counter() - t0
+        done += n
+        n = min(n * 2, max_entries - done) if done < max_entries else 0
+        if n <= 0:
+            break
+    return {"value": done / spent, "unit": "entries/s", "cores": os.cpu_count(), "kind": "reference",
+            "sample": "%d seeded random entries (%d rays each), reference kernel code built for the host, "
+                      "OpenMP over entries, %.1f s" % (done, p.rays_per_entry, spent)}
+
+
+def run_reference_impl(args, world, rank):
+    if rank != 0:
+        return
+    p = pe_workload(args.workload)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_py
+    if not oracle_py.ref_available("pe_f32"):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libref_pe_f32.so not built (no reference tree at build time)"}))
+        return
+    rng = np.random.default_rng(1)
+    per_step = args.ref_entries
+    for _ in range(args.warmup):
+        oracle_py.ref_pe_entries(p, rng.integers(0, p.n_crystals, per_step), rng.integers(0, p.n_voxels, per_step))
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        oracle_py.ref_pe_entries(p, rng.integers(0, p.n_crystals, per_step), rng.integers(0, p.n_voxels, per_step))
+    dt = time.perf_counter() - t0
+    value = args.steps * per_step / dt
+    sample = ("%d seeded random entries per step of %s (%d rays each), reference kernel code built for the host, "
+              "OpenMP over entries" % (per_step, args.workload, p.rays_per_entry))
+    line = {"metric": "pe sysmat entries/s", "value": value, "unit": "entries/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded %s geometry)" % args.workload, "impl": "reference",
+            "config": {"workload": args.workload, "crystals": p.n_crystals, "voxels": p.n_voxels,
+                       "rays_per_entry": p.rays_per_entry, "step": "bounded sample of entries"},
+            "cpu_baseline": {"value": value, "unit": "entries/s", "cores": os.cpu_count(), "kind": "reference",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": "entries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+# ---------------------------------------------------------------------------
+# GPU: the reference's CUDA kernel on this GPU (bounded sample)
+# ---------------------------------------------------------------------------
+
+def ref_cuda_rate(p, device: int, n_rows: int = 64):
+    """The reference's photodetectorCudaMe (built for sm_100a with this
+    workload's crystal sub-cells) on a seeded random set of n_rows crystals
+    (moved to the front of the detector table) and one fine slab of 4 planes
+    of the k-times finer voxel grid that emulates voxel sub-sampling."""
+    import torch
+    path = os.path.join(ROOT, "oracle", "_ref", "libref_pe_cuda_%dx%dx%d.so" % tuple(p.sc))
+    if not os.path.exists(path):
+        return {"unavailable": "%s not built" % os.path.basename(path)}
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_py
+    lib = ctypes.CDLL(path)
+    lib.ref_cuda_pe_kernel.restype = ctypes.c_int
+    rng = np.random.default_rng(5)
+    N = p.n_crystals
+    pick = rng.choice(N, n_rows, replace=False)
+    order = np.concatenate([pick, np.setdiff1d(np.arange(N), pick)])
+    det = np.zeros(max(80000, p.detector.size), np.float32)
+    det[0] = N
+    body = p.detector[1:1 + 12 * N].reshape(N, 12)[order]
+    det[1:1 + 12 * N] = body.ravel()
+    col = np.zeros(max(80000, p.collimator.size), np.float32)
+    col[:p.collimator.size] = p.collimator
+    img = oracle_py.fine_image(p)
+    fnz = int(img[2])
+    z0 = fnz // 2 - SLAB_Z // 2
+    img[30] = fnz
+    img[31] = z0
+    img[2] = SLAB_Z
+    img[20] = 0
+    cells = int(img[0]) * int(img[1]) * SLAB_Z
+    dev = torch.device("cuda", device)
+    d_col = torch.from_numpy(col).to(dev)
+    d_det = torch.from_numpy(det).to(dev)
+    d_img = torch.from_numpy(img).to(dev)
+    d_dst = torch.zeros(n_rows * cells, dtype=torch.float32, device=dev)
+    ms = ctypes.c_float(0)
+    fp = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+    rc = lib.ref_cuda_pe_kernel(fp(d_col), fp(d_det), fp(d_img), fp(d_dst), n_rows, cells, 1, ctypes.byref(ms))
+    if rc != 0:
+        return {"unavailable": "reference kernel returned CUDA error %d" % rc}
+    rc = lib.ref_cuda_pe_kernel(fp(d_col), fp(d_det), fp(d_img), fp(d_dst), n_rows, cells, 1, ctypes.byref(ms))
+    n_sv = int(np.prod(p.sv))
+    entries = n_rows * cells / n_sv
+    return {"value": entries / (ms.value / 1e3), "unit": "entries/s", "kernel_ms": ms.value,
+            "sample": "%d random crystals x one %d-plane slab of the %dx finer grid (%d fine cells = %d entries of "
+                      "%d rays); reference launch shape 16x32" % (n_rows, SLAB_Z, p.sv[0], n_rows * cells,
+                                                                   int(entries), p.rays_per_entry)}
+
+
+# ---------------------------------------------------------------------------
+# Our kernel
+# ---------------------------------------------------------------------------
+
+def run_ours(args, world, rank, local):
+    import torch
+    import sysmat_b200
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=dev)
+    p = pe_workload(args.workload)
+    ctx = sysmat_b200.Context(local)
+    geo = sysmat_b200.Geometry(ctx, p)
+    nx, ny, nz = p.grid
+    n_slabs = nz // SLAB_Z
+    slab_vox = nx * ny * SLAB_Z
+    rows = p.n_crystals
+    out = torch.empty((rows, slab_vox), dtype=torch.float32, device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.Stream(device=dev)
+    opts = geo.options()
+
+    def step(i):
+        s = (i * world + rank) % n_slabs
+        flush.zero_()
+        geo.pe(z=(s * SLAB_Z, SLAB_Z), opts=opts, out=out.data_ptr(), stream=stream.cuda_stream)
+
+    with torch.cuda.stream(stream):
+        for i in range(args.warmup):
+            step(i)
+    ctx.sync(stream.cuda_stream)
+    torch.cuda.synchronize()
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        with torch.cuda.stream(stream):
+            t_start.record(stream)
+            for i in range(args.steps):
+                s = (i * world + rank) % n_slabs
+                flush.zero_()
+                starts[i].record(stream)
+                geo.pe(z=(s * SLAB_Z, SLAB_Z), opts=opts, out=out.data_ptr(), stream=stream.cuda_stream)
+                ends[i].record(stream)
+            t_end.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    ctx.sync(stream.cuda_stream)
+    total_ms = t_start.elapsed_time(t_end)
+    kernel_ms = [a.elapsed_time(b) for a, b in zip(starts, ends)]
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([total_ms, sum(kernel_ms)], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms, kernel_sum = float(t[0]), float(t[1])
+    else:
+        kernel_sum = sum(kernel_ms)
+    entries_per_step = rows * slab_vox
+    value = world * args.steps * entries_per_step / (total_ms / 1e3)
+
+    # Work counters of one slab (separate, counted run).
+    ctx.set_counters(True)
+    geo.pe(z=(0, SLAB_Z), opts=opts, out=out.data_ptr(), stream=stream.cuda_stream)
+    n_rays, n_cry, n_hole, n_cone = ctx.last_counters()
+    ctx.set_counters(False)
+    flops = (n_rays * (F_RAY + p.n_plates * F_BOX + 2 * F_IN + F_BOX) + n_cry * (F_BOX + F_XF) + n_hole * F_CYL
+             + n_cone * F_CONE)
+    kernel_s = kernel_sum / args.steps / 1e3
+    peaks, peak_src = load_peaks()
+    sm_max = float(peaks.get("sm_max_mhz", 1965.0))
+    fp32_peak = 148 * 128 * 2 * sm_max * 1e6 / 1e12
+    achieved = flops / kernel_s / 1e12
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "pe_trace_kernel_traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            tr = json.load(f)
+        traffic = tr.get("bytes_per_entry", 0.0) * entries_per_step
+
+    # End to end through the public API: tables in from host memory, slab out to pinned host memory.
+    e2e = None
+    if args.e2e_steps > 0:
+        host = torch.empty((rows, slab_vox), dtype=torch.float32, pin_memory=True).numpy()
+        barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for i in range(args.e2e_steps):
+            s = (i * world + rank) % n_slabs
+            g2 = sysmat_b200.Geometry(ctx, p)
+            g2.pe(z=(s * SLAB_Z, SLAB_Z), opts=opts, out=host)
+            g2.close()
+        torch.cuda.synchronize()
+        e2e_s = time.perf_counter() - t0
+        if world > 1:
+            import torch.distributed as dist
+            t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_s = float(t[0])
+        e2e = {"value": world * args.e2e_steps * entries_per_step / e2e_s, "unit": "entries/s",
+               "h2d_bytes_per_step": 4 * (p.collimator.size + p.detector.size + p.image.size + p.physics.size),
+               "d2h_bytes_per_step": 4 * rows * slab_vox, "steps": args.e2e_steps,
+               "path": "sysmat_b200.Geometry(tables) + Geometry.pe(host out) per step"}
+
+    if rank == 0:
+        line = {
+            "metric": "pe sysmat entries/s", "value": value, "unit": "entries/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded %s geometry)" % args.workload,
+            "config": {"workload": args.workload, "crystals": rows, "voxels": p.n_voxels, "holes": p.n_holes,
+                       "plates": p.n_plates, "sv": list(p.sv), "sc": list(p.sc), "rays_per_entry": p.rays_per_entry,
+                       "step": "one %d-plane z-slab x all crystals (%d entries)" % (SLAB_Z, entries_per_step),
+                       "l2": "flushed between steps (%d MiB memset)" % (L2_FLUSH_BYTES >> 20),
+                       "parallelism": "slabs sharded across ranks, no data-path collective"},
+            "rays_per_s": value * p.rays_per_entry,
+            "kernel_ms_per_step": kernel_sum / args.steps,
+            "gpu_launches": args.steps,
+            "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+                         "frac": achieved / fp32_peak, "traffic": traffic,
+                         "peak_source": "FP32 issue peak 148 SMs x 128 lanes x 2 FLOP x sm_max %.0f MHz (%s clock)" % (sm_max, peak_src.split()[1]),
+                         "work": {"rays": n_rays, "exact_crystal_tests": n_cry, "exact_hole_tests": n_hole,
+                                  "cone_tests": n_cone, "flops_per_step": flops},
+                         "hbm_write_gbs": 4 * entries_per_step / kernel_s / 1e9,
+                         "hbm_frac": 4 * entries_per_step / kernel_s / 1e9 / float(peaks.get("hbm_gbs", 6650.0))},
+            "clocks": clocks.summary(),
+        }
+        if e2e:
+            line["e2e"] = e2e
+        if not args.no_ref_cuda:
+            try:
+                line["ref_cuda"] = ref_cuda_rate(p, local)
+            except Exception as exc:  # the reference kernel is a baseline, not the product
+                line["ref_cuda"] = {"unavailable": "%s" % exc}
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_reference_rate(p, args.cpu_seconds)
+        print(json.dumps(line))
+    geo.close()
+    ctx.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=8)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default="pe_large")
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--ref-entries", type=int, default=4096)
+    ap.add_argument("--no-ref-cuda", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        run_reference_impl(args, world, rank)
+    else:
+        run_ours(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    main()

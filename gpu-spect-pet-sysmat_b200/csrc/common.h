@@ -1,0 +1,38 @@
+// Shared host-side helpers: status codes, thread-local error message, CUDA checks.
+#pragma once
+
+#include <cstdarg>
+#include <cstdio>
+#include <string>
+
+#include <cuda_runtime.h>
+
+#include "sysmat_b200.h"
+
+namespace smb {
+
+// Records `fmt` as the calling thread's last error and returns `code`.
+int fail(int code, const char* fmt, ...);
+const char* last_error();
+
+struct CudaError {
+    int code;
+};
+
+// Returns SM_ERR_CUDA with the runtime's message when `e` is not cudaSuccess.
+inline int check_cuda(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return SM_OK;
+    if (e == cudaErrorMemoryAllocation)
+        return fail(SM_ERR_ALLOC, "%s: %s", what, cudaGetErrorString(e));
+    return fail(SM_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define SM_TRY(expr)                      \
+    do {                                  \
+        int sm_try_rc_ = (expr);          \
+        if (sm_try_rc_ != SM_OK) return sm_try_rc_; \
+    } while (0)
+
+#define SM_CUDA(expr) SM_TRY(::smb::check_cuda((expr), #expr))
+
+}  // namespace smb

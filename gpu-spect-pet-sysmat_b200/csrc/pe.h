@@ -1,0 +1,66 @@
+// Photoelectric sysmat kernel: launch parameters and host launcher.
+#pragma once
+
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+#include "geometry.h"
+
+namespace smb {
+
+constexpr int kPeWarps = 8;            // warps per CTA = crystals per tile
+constexpr int kPeThreads = 32 * kPeWarps;
+constexpr int kSupC = 512;             // tile superset capacity, crystals
+constexpr int kSupH = 256;             // tile superset capacity, holes
+constexpr int kMaxGroup = 4;           // voxel sub-points whose candidate masks are live at once
+constexpr int kMaxTileVoxels = 128;    // voxels per brick
+constexpr int kRecHoles = 16;          // hit-record capacity per ray
+constexpr int kRecCrystals = 40;
+constexpr int kRecWords = 3 + kRecHoles + kRecCrystals;
+
+// Bits of the device status word.
+enum : int {
+    kStatusSupersetOverflow = 1,
+    kStatusRecordOverflow = 2,
+};
+
+struct PEParams {
+    int nx, ny, nz;          // coarse grid (full volume)
+    int z0, nzs;             // slab: coarse z range [z0, z0 + nzs)
+    int kx, ky, kz;          // voxel sub-samples
+    int fnx, fny, fnz;       // fine grid = coarse * k
+    float fvx, fvy, fvz;     // fine voxel size = voxel / k (float division)
+    float shx, shy, shz;     // FOV shift
+    float cos_a, sin_a;      // image rotation about z
+    int dX, dY, dZ;          // crystal sub-cells
+    int n_sc, n_sv, group;   // sub-cells per crystal, sub-points per voxel, sub-points per mask group
+    float inv_sv;
+    int row0, row1;          // crystal rows [row0, row1)
+    int bx, by, bz;          // voxel brick
+    int tiles_x, tiles_y, tiles_z;
+    int n_ctiles;            // crystal tiles
+    long long n_tiles;       // total tiles = n_ctiles * tiles_x * tiles_y * tiles_z
+    const long long* tile_list;   // optional explicit tile ids (record mode)
+    float* dst;
+    long long ld;
+    int* status;
+    unsigned long long* counters; // optional: rays, exact crystal tests, exact hole tests, cone tests
+    // record mode
+    int rec_n;
+    const long long* rec_rows;
+    const long long* rec_vox;    // full-volume coarse voxel index
+    int* rec_out;
+};
+
+// Fills every field of `p` but the output, status and record pointers, for the
+// slab [z0, z0 + nz) of a volume of nz_full z-planes and rows [row0, row1).
+void pe_plan(const HostGeometry& g, const int sv[3], const int sc[3], const int brick[3], int rotation,
+             int row0, int row1, int nz_full, int z0, int nz, PEParams* p);
+
+// Launches the trace kernel (RECORD selects the hit-recording instantiation).
+cudaError_t pe_launch(const PEParams& p, const DevGeometry& geo, bool record, long long n_tiles, cudaStream_t stream);
+
+size_t pe_smem_bytes();
+
+}  // namespace smb

@@ -1,0 +1,258 @@
+"""sysmat_b200: ctypes binding of libsysmat_b200.so (B200 / sm_100a).
+
+The C ABI is declared in ``include/sysmat_b200.h``.  This module mirrors it:
+
+* :func:`PESysMatGen` -- the reference's entry point
+  (``PEGen_RayTracing_CircularHole/PESysMatGen.h:4-9``): host tables, host
+  ``dst`` of one z-slab, returns the number of voxels per row.
+* :class:`Context`, :class:`Geometry` and :meth:`Geometry.pe` -- the
+  status-returning API with explicit sub-sampling, row ranges, slabs, host or
+  device outputs and caller streams.
+
+There is no fallback: if the shared library is missing or no sm_100 device is
+present, calls raise :class:`SysmatError`.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional, Sequence, Tuple
+
+import numpy as np
+
+from . import params as params  # noqa: F401  (re-export)
+from . import configs as configs  # noqa: F401
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libsysmat_b200.so")
+
+SM_OK = 0
+ERRORS = {-1: "SM_ERR_INVALID", -2: "SM_ERR_CAPACITY", -3: "SM_ERR_CUDA", -4: "SM_ERR_ALLOC",
+          -5: "SM_ERR_IO", -6: "SM_ERR_TIMEOUT", -7: "SM_ERR_DEVICE"}
+
+
+class SysmatError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__("%s (%d): %s" % (ERRORS.get(code, "SM_ERR"), code, message))
+        self.code = code
+
+
+class PeOptions(ctypes.Structure):
+    _fields_ = [("sv", ctypes.c_int * 3), ("sc", ctypes.c_int * 3), ("tile_voxels", ctypes.c_int * 3),
+                ("flags", ctypes.c_int)]
+
+    @staticmethod
+    def make(sv=(1, 1, 1), sc=(8, 16, 8), tile_voxels=(0, 0, 0)) -> "PeOptions":
+        o = PeOptions()
+        for i in range(3):
+            o.sv[i], o.sc[i], o.tile_voxels[i] = int(sv[i]), int(sc[i]), int(tile_voxels[i])
+        o.flags = 0
+        return o
+
+
+_lib = None
+_f32p = ctypes.POINTER(ctypes.c_float)
+_i64p = ctypes.POINTER(ctypes.c_int64)
+_i32p = ctypes.POINTER(ctypes.c_int32)
+_vp = ctypes.c_void_p
+
+# Prototypes of every exported function: (restype, argtypes).
+PROTOTYPES = {
+    "PESysMatGen": (ctypes.c_int, [_f32p, _f32p, _f32p, _f32p, ctypes.c_int]),
+    "scatter": (ctypes.c_int, [_f32p, _f32p, _f32p, _f32p, _f32p, ctypes.c_char_p, ctypes.c_char_p, _f32p,
+                               ctypes.c_int]),
+    "sm_last_error": (ctypes.c_char_p, []),
+    "sm_version": (ctypes.c_char_p, []),
+    "sm_context_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(_vp)]),
+    "sm_context_destroy": (ctypes.c_int, [_vp]),
+    "sm_context_sync": (ctypes.c_int, [_vp, _vp]),
+    "sm_geometry_create": (ctypes.c_int, [_vp, _f32p, ctypes.c_size_t, _f32p, ctypes.c_size_t, _f32p,
+                                          ctypes.c_size_t, _f32p, ctypes.c_size_t, ctypes.POINTER(_vp)]),
+    "sm_geometry_destroy": (ctypes.c_int, [_vp]),
+    "sm_geometry_info": (ctypes.c_int, [_vp, _i64p]),
+    "sm_pe_options_reference": (None, [ctypes.POINTER(PeOptions)]),
+    "sm_pe_compute": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(PeOptions), ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                     ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int64, ctypes.c_int, _vp]),
+    "sm_pe_record_hits": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(PeOptions), ctypes.c_int, _i64p, _i64p,
+                                         ctypes.c_int64, _i32p, ctypes.POINTER(ctypes.c_int)]),
+    "sm_pe_set_counters": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "sm_pe_last_counters": (ctypes.c_int, [_vp, _i64p]),
+    "sm_primitive_batch": (ctypes.c_int, [ctypes.c_int, _f32p, ctypes.c_int64, _f32p]),
+}
+
+
+def lib():
+    """Load libsysmat_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise SysmatError(-7, "%s is missing: build it with `make -C gpu-spect-pet-sysmat_b200/csrc`" % LIB_PATH)
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in PROTOTYPES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _check(rc: int):
+    if rc != SM_OK:
+        raise SysmatError(rc, (lib().sm_last_error() or b"").decode(errors="replace"))
+
+
+def _fptr(a: np.ndarray):
+    return a.ctypes.data_as(_f32p)
+
+
+def _as_f32(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+# --------------------------------------------------------------------------
+# Reference interface
+# --------------------------------------------------------------------------
+
+def PESysMatGen(parameter_Collimator, parameter_Detector, parameter_Image, dst: np.ndarray, cuda_id: int = 0) -> int:
+    """Drop-in for the reference's ``int PESysMatGen(float*, float*, float*, float*, int)``.
+
+    ``parameter_Image`` carries the slab side channel ([2] slab nz, [30] full
+    nz, [31] z0, [20] rotation index) exactly as the reference's CLI sets it.
+    ``dst`` (float32, C-contiguous) receives [N][nx*ny*Image[2]].  Tables must
+    hold at least 80000 / 80000 / 100 floats.
+    """
+    col, det, img = _as_f32(parameter_Collimator), _as_f32(parameter_Detector), _as_f32(parameter_Image)
+    if col.size < 80000 or det.size < 80000 or img.size < 100:
+        raise SysmatError(-1, "PESysMatGen reads 80000 / 80000 / 100 floats")
+    if not (dst.dtype == np.float32 and dst.flags.c_contiguous):
+        raise SysmatError(-1, "dst must be a C-contiguous float32 array")
+    return lib().PESysMatGen(_fptr(col), _fptr(det), _fptr(img), _fptr(dst), int(cuda_id))
+
+
+# --------------------------------------------------------------------------
+# Status-returning API
+# --------------------------------------------------------------------------
+
+class Context:
+    def __init__(self, device: int = 0):
+        h = _vp()
+        _check(lib().sm_context_create(int(device), ctypes.byref(h)))
+        self.handle = h
+        self.device = device
+
+    def close(self):
+        if self.handle:
+            lib().sm_context_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def sync(self, stream: int = 0):
+        _check(lib().sm_context_sync(self.handle, _vp(stream)))
+
+    def set_counters(self, enable: bool):
+        _check(lib().sm_pe_set_counters(self.handle, 1 if enable else 0))
+
+    def last_counters(self) -> Tuple[int, int, int, int]:
+        out = np.zeros(4, dtype=np.int64)
+        _check(lib().sm_pe_last_counters(self.handle, out.ctypes.data_as(_i64p)))
+        return tuple(int(x) for x in out)
+
+
+class Geometry:
+    """Parsed, validated, device-resident geometry built from the four tables."""
+
+    def __init__(self, ctx: Context, p):
+        self.ctx = ctx
+        self.params = p
+        self._tables = [_as_f32(p.collimator), _as_f32(p.detector), _as_f32(p.image), _as_f32(p.physics)]
+        col, det, img, phy = self._tables
+        h = _vp()
+        _check(lib().sm_geometry_create(ctx.handle, _fptr(col), col.size, _fptr(det), det.size, _fptr(img), img.size,
+                                        _fptr(phy), phy.size, ctypes.byref(h)))
+        self.handle = h
+        info = np.zeros(7, dtype=np.int64)
+        _check(lib().sm_geometry_info(h, info.ctypes.data_as(_i64p)))
+        self.n_crystals, self.n_holes, self.n_plates, self.nx, self.ny, self.nz, self.n_rotations = map(int, info)
+
+    def close(self):
+        if self.handle:
+            lib().sm_geometry_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def options(self, sv=None, sc=None, tile_voxels=(0, 0, 0)) -> PeOptions:
+        sv = self.params.sv if sv is None else sv
+        sc = self.params.sc if sc is None else sc
+        return PeOptions.make(sv, sc, tile_voxels)
+
+    def pe(self, rotation: int = 0, rows: Optional[Tuple[int, int]] = None, z: Optional[Tuple[int, int]] = None,
+           opts: Optional[PeOptions] = None, out=None, ld: Optional[int] = None, stream: int = 0) -> np.ndarray:
+        """Photoelectric sysmat block [rows][slab voxels].
+
+        ``out`` may be None (a host array is returned), a host float32 array,
+        or an integer device pointer (the call is then asynchronous on
+        ``stream`` and returns None).
+        """
+        r0, r1 = rows if rows is not None else (0, self.n_crystals)
+        z0, nz = z if z is not None else (0, self.nz)
+        opts = opts if opts is not None else self.options()
+        slab = self.nx * self.ny * nz
+        ld = slab if ld is None else ld
+        if out is None or isinstance(out, np.ndarray):
+            host = np.zeros((r1 - r0, ld), dtype=np.float32) if out is None else out
+            if host.dtype != np.float32 or not host.flags.c_contiguous or host.size < (r1 - r0) * ld:
+                raise SysmatError(-1, "out must be C-contiguous float32 with rows*ld elements")
+            _check(lib().sm_pe_compute(self.ctx.handle, self.handle, ctypes.byref(opts), int(rotation), int(r0),
+                                       int(r1), int(z0), int(nz), _vp(host.ctypes.data), int(ld), 0, _vp(stream)))
+            return host
+        _check(lib().sm_pe_compute(self.ctx.handle, self.handle, ctypes.byref(opts), int(rotation), int(r0), int(r1),
+                                   int(z0), int(nz), _vp(int(out)), int(ld), 1, _vp(stream)))
+        return None
+
+    def record_hits(self, rows: Sequence[int], voxels: Sequence[int], rotation: int = 0,
+                    opts: Optional[PeOptions] = None) -> np.ndarray:
+        """Per-ray hit records of entries (rows[i], voxels[i]); shape (n, rays, words)."""
+        opts = opts if opts is not None else self.options()
+        r = np.ascontiguousarray(rows, dtype=np.int64)
+        v = np.ascontiguousarray(voxels, dtype=np.int64)
+        rays = int(np.prod(opts.sv)) * int(np.prod(opts.sc))
+        words = ctypes.c_int(0)
+        out = np.zeros(r.size * rays * 64, dtype=np.int32)
+        _check(lib().sm_pe_record_hits(self.ctx.handle, self.handle, ctypes.byref(opts), int(rotation),
+                                       r.ctypes.data_as(_i64p), v.ctypes.data_as(_i64p), r.size,
+                                       out.ctypes.data_as(_i32p), ctypes.byref(words)))
+        w = words.value
+        return out[:r.size * rays * w].reshape(r.size, rays, w)
+
+
+def primitive_batch(kind: str, args: np.ndarray) -> np.ndarray:
+    """Run the device ray primitives (``box``, ``inside``, ``cylinder``) on argument rows."""
+    k = {"box": 0, "inside": 1, "cylinder": 2}[kind]
+    a = _as_f32(args)
+    n = a.shape[0]
+    out = np.zeros(n, dtype=np.float32)
+    _check(lib().sm_primitive_batch(k, _fptr(a), n, _fptr(out)))
+    return out
+
+
+def parse_records(rec: np.ndarray, n_holes_cap: int = 16):
+    """Decode one entry's records (rays, words) into {ray: (plate_mask, holes, crystals)}."""
+    out = {}
+    for ray in range(rec.shape[0]):
+        w = rec[ray]
+        nh = int(w[1])
+        holes = tuple(int(x) for x in w[2:2 + nh])
+        nc = int(w[2 + n_holes_cap])
+        crystals = tuple(int(x) for x in w[3 + n_holes_cap:3 + n_holes_cap + nc])
+        out[ray] = (int(w[0]), holes, crystals)
+    return out

@@ -1,0 +1,142 @@
+/* sysmat_b200 -- B200 (sm_100a) SPECT/PET system-matrix generator, C ABI.
+ *
+ * Two layers of entry points:
+ *
+ * 1. Legacy drop-ins with the reference's exact signatures and semantics
+ *    (host buffers, tables of at least 80000 / 80000 / 100 / 100 floats,
+ *    return value = voxels per row, device chosen per call):
+ *      PESysMatGen   replaces PEGen_RayTracing_CircularHole/PESysMatGen.h:4-9
+ *      scatter       replaces ScatterGen_RayTracing_CircularHole/scatter.h:4-5
+ *    The crystal-only and collimator-only `scatter` variants of
+ *    ScatterGen_Crystal/scatter.h:4 and ScatterGen_Collimator/scatter.h:4-5 share
+ *    the symbol name, so they live in the two small shim libraries
+ *    libsysmat_b200_scatter_crystal.so / libsysmat_b200_scatter_collimator.so.
+ *    Unlike the reference, they never call exit(): on failure they print the
+ *    reason to stderr and return -1.
+ *
+ * 2. The status-returning sm_* API: explicit table lengths, sub-sampling
+ *    options, device or host outputs, a caller stream, and no process exit.
+ *    Every sm_* function returns SM_OK (0) or a negative SM_ERR_* code;
+ *    sm_last_error() gives the message of the calling thread's last failure.
+ *
+ * Conventions: tables are the reference's float32 Params layouts (Y = depth);
+ * sysmat rows are crystals, columns are voxels x + nx*(y + ny*z); a "slab" is the
+ * voxel range z in [z0, z0 + nz) and occupies nx*ny*nz consecutive columns.
+ */
+#ifndef SYSMAT_B200_H
+#define SYSMAT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- legacy drop-ins ------------------------------------------------------ */
+
+/* PEGen_RayTracing_CircularHole/PESysMatGen.h:4-9 and PESysMatGen.cu:766-833.
+ * Computes the photoelectric sysmat of one z-slab for rotation Image[20]:
+ * rows = all crystals, columns = the slab of Image[2] z-planes starting at
+ * Image[31] in a volume of Image[30] z-planes.  dst is host memory of
+ * N * nx * ny * Image[2] floats.  Crystal sub-cells 8 x 16 x 8, voxel centre
+ * only, as the reference.  Returns nx * ny * Image[2], or -1 on failure. */
+int PESysMatGen(float* parameter_Collimator, float* parameter_Detector, float* parameter_Image,
+                float* dst, int cuda_id);
+
+/* ScatterGen_RayTracing_CircularHole/scatter.h:4-5 and scatter.cu:2013-2378.
+ * Primary Compton scatter (crystal + collimator parts) for rotation Image[20];
+ * PE_SysMat is the host PE sysmat of that rotation ([N][V]); dst receives
+ * [N][V].  Physics[8] / Physics[9] == 1 compute the geometry bitmaps and write
+ * them to FnameGeoCrystal / FnameGeoCollimator, otherwise they are read from
+ * those files.  Returns V, or -1 on failure. */
+int scatter(float* parameter_Collimator, float* parameter_Detector, float* parameter_Image,
+            float* parameter_Physics, float* PE_SysMat, const char* FnameGeoCrystal,
+            const char* FnameGeoCollimator, float* dst, int cuda_id);
+
+/* ---- status codes ---------------------------------------------------------- */
+enum {
+    SM_OK = 0,
+    SM_ERR_INVALID = -1,     /* bad argument or malformed table            */
+    SM_ERR_CAPACITY = -2,    /* a table or tile exceeds a supported size   */
+    SM_ERR_CUDA = -3,        /* CUDA runtime error                         */
+    SM_ERR_ALLOC = -4,       /* device or host allocation failed           */
+    SM_ERR_IO = -5,          /* file open/read/write failed                */
+    SM_ERR_TIMEOUT = -6,     /* a bounded device-side wait expired         */
+    SM_ERR_DEVICE = -7       /* no usable sm_100 device                    */
+};
+
+const char* sm_last_error(void);
+const char* sm_version(void);
+
+/* ---- context and geometry -------------------------------------------------- */
+typedef struct sm_context sm_context;
+typedef struct sm_geometry sm_geometry;
+
+/* Binds a CUDA device (cudaSetDevice on every call that launches work). */
+int sm_context_create(int device, sm_context** out);
+int sm_context_destroy(sm_context* ctx);
+/* Waits for `stream` and reports any device-side status raised by kernels of
+ * this context since the last check (e.g. SM_ERR_CAPACITY). */
+int sm_context_sync(sm_context* ctx, void* stream);
+
+/* Parses and validates the four tables (lengths in floats), uploads the
+ * derived structure-of-arrays geometry to the context's device once.
+ * Validation errors name the offending field. */
+int sm_geometry_create(sm_context* ctx, const float* collimator, size_t n_collimator,
+                       const float* detector, size_t n_detector, const float* image, size_t n_image,
+                       const float* physics, size_t n_physics, sm_geometry** out);
+int sm_geometry_destroy(sm_geometry* geo);
+/* n_crystals, n_holes, n_plates, nx, ny, nz, n_rotations */
+int sm_geometry_info(const sm_geometry* geo, int64_t out[7]);
+
+/* ---- photoelectric sysmat -------------------------------------------------- */
+typedef struct sm_pe_options {
+    int sv[3];          /* voxel sub-samples (x, y, z); the entry is their mean  */
+    int sc[3];          /* crystal sub-cells (x, y = depth, z); summed           */
+    int tile_voxels[3]; /* voxel brick per CTA; 0 = autotuned / default          */
+    int flags;          /* reserved, 0                                           */
+} sm_pe_options;
+
+/* Reference mode: sv = 1x1x1, sc = 8x16x8 (PESysMatGen.cu:435-440). */
+void sm_pe_options_reference(sm_pe_options* opt);
+
+/* Photoelectric sysmat for rows [row0, row1) and the voxel slab z in
+ * [z0, z0 + nz) of rotation `rotation`.  dst[(r - row0) * ld + c] receives
+ * column c of the slab (c < nx*ny*nz); ld >= nx*ny*nz.  dst is a device
+ * pointer when dst_on_device != 0 (the call is asynchronous on `stream`),
+ * otherwise host memory (the call copies and synchronises).  stream may be
+ * NULL (legacy default stream). */
+int sm_pe_compute(sm_context* ctx, const sm_geometry* geo, const sm_pe_options* opt, int rotation,
+                  int row0, int row1, int z0, int nz, float* dst, int64_t ld, int dst_on_device,
+                  void* stream);
+
+/* Diagnostic: for each listed entry (rows[i], voxels[i] as full-volume voxel
+ * index) record every ray's hits exactly as the production kernel decides
+ * them.  Per ray, `record_words` int32: [plate-miss mask, n_holes, holes
+ * (<= 16), n_crystals, crystals (<= 40)], ids ascending; rays in the order
+ * sub-point (x fastest, then y, z) x sub-cell (depth fastest, then x, then
+ * z).  out (host) holds n * rays_per_entry * record_words int32. */
+int sm_pe_record_hits(sm_context* ctx, const sm_geometry* geo, const sm_pe_options* opt,
+                      int rotation, const int64_t* rows, const int64_t* voxels, int64_t n,
+                      int32_t* out, int* record_words);
+
+/* Work counters: when enabled, each sm_pe_compute on the context counts rays
+ * traced, exact crystal tests, exact hole tests and candidate cone tests
+ * (costs a little time and synchronises the call). */
+int sm_pe_set_counters(sm_context* ctx, int enable);
+int sm_pe_last_counters(sm_context* ctx, int64_t out[4]);
+
+/* Diagnostic: evaluate the tracer's ray primitives on the current device for
+ * n argument rows (host arrays).  kind 0: chord through a box (12 floats:
+ * segment in, out, box min, max), 1: chord from box entry to segment end
+ * (12 floats), 2: chord through a hole cylinder (11 floats: in, out, x, y1,
+ * y2, z, R).  Same device code as the sysmat kernel; replaces no reference
+ * interface (the reference's primitives are PESysMatGen.cu:19-373). */
+int sm_primitive_batch(int kind, const float* args, int64_t n, float* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SYSMAT_B200_H */

@@ -478,7 +478,23 @@ long long oracle_pe_hits(const float* col, const float* det, const float* img, c
     return n;
 }
 
-/* Primitive batches (float arithmetic), for the primitive-level pin against the reference. */
+/* Primitive batches for the primitive-level pins: float arithmetic (the
+ * reference's), and dual (single-precision decisions, double magnitudes). */
+int oracle_box_ray_batch_dual(const float* a, long long n, double* out) {
+    for (long long i = 0; i < n; ++i, a += 12)
+        out[i] = chord_through<Dual>(a[0], a[1], a[2], a[3], a[4], a[5], a[6], a[7], a[8], a[9], a[10], a[11]).d;
+    return 0;
+}
+int oracle_box_inside_batch_dual(const float* a, long long n, double* out) {
+    for (long long i = 0; i < n; ++i, a += 12)
+        out[i] = chord_to_end<Dual>(a[0], a[1], a[2], a[3], a[4], a[5], a[6], a[7], a[8], a[9], a[10], a[11]).d;
+    return 0;
+}
+int oracle_cylinder_batch_dual(const float* a, long long n, double* out) {
+    for (long long i = 0; i < n; ++i, a += 11)
+        out[i] = chord_hole<Dual>(a[0], a[1], a[2], a[3], a[4], a[5], a[6], a[7], a[8], a[9], a[10]).d;
+    return 0;
+}
 int oracle_box_ray_batch(const float* a, long long n, double* out) {
     for (long long i = 0; i < n; ++i, a += 12)
         out[i] = chord_through<float>(a[0], a[1], a[2], a[3], a[4], a[5], a[6], a[7], a[8], a[9], a[10], a[11]);

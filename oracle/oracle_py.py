@@ -177,9 +177,12 @@ def _batch(libfn, args: np.ndarray, width: int) -> np.ndarray:
 
 
 def primitive(kind: str, args: np.ndarray, impl: str = "oracle") -> np.ndarray:
-    """kind in {box, inside, cylinder}; impl 'oracle' or 'ref'."""
+    """kind in {box, inside, cylinder}; impl 'oracle' (float), 'dual' (float
+    decisions, double values) or 'ref' (the reference's own primitives)."""
     width = 11 if kind == "cylinder" else 12
     name = {"box": "box_ray_batch", "inside": "box_inside_batch", "cylinder": "cylinder_batch"}[kind]
     if impl == "oracle":
         return _batch(getattr(oracle_lib(), "oracle_" + name), args, width)
+    if impl == "dual":
+        return _batch(getattr(oracle_lib(), "oracle_" + name + "_dual"), args, width)
     return _batch(getattr(ref_lib("pe_f32"), "ref_" + name), args, width)

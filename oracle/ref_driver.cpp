@@ -44,30 +44,44 @@ static std::vector<real> widen(const float* src, int64_t n, int64_t min_len) {
 
 extern "C" {
 
-/* Evaluate the reference PE kernel for cells (rows[i], cols[i]).
- * `img` must already carry the slab side channel: img[2] = slab nz,
- * img[30] = full nz, img[31] = slab z0, img[20] = rotation index.
- * n_cols_total is numImagebin (voxels in the slab). */
+/* Evaluate the reference PE kernel for cells (rows[i], cols[i]), where
+ * cols[i] indexes the full volume described by img[0..2].  Each cell is run
+ * as the reference CLI runs it: as part of the one-plane slab that contains
+ * it (img[2] = 1, img[30] = full nz, img[31] = the cell's z), so the
+ * kernel's 32-bit index row * numImagebin + col stays in range
+ * (PEGen_CircularHole.cpp:181-194, PESysMatGen.cu:424). */
 int ref_pe_entries(const float* col, int64_t ncol, const float* det, int64_t ndet,
                    const float* img, int divx, int divy, int divz,
                    int n_rows_total, int n_cols_total,
                    const int64_t* rows, const int64_t* cols, int64_t n,
                    double* out, int nthreads)
 {
-    std::vector<real> c = widen(col, ncol, 80000), d = widen(det, ndet, 80000), im = widen(img, 100, 100);
+    (void)n_cols_total;
+    std::vector<real> c = widen(col, ncol, 80000), d = widen(det, ndet, 80000);
+    const int nx = (int)img[0], ny = (int)img[1], nz = (int)img[2];
+    const int plane = nx * ny;
     if (nthreads <= 0) nthreads = omp_get_max_threads();
-#pragma omp parallel for schedule(dynamic, 8) num_threads(nthreads)
-    for (int64_t i = 0; i < n; ++i) {
-        ref_div[0] = (unsigned)divx; ref_div[1] = (unsigned)divy; ref_div[2] = (unsigned)divz;
-        blockDim = {1u, 1u, 1u};
-        threadIdx = {0u, 0u, 0u};
-        blockIdx = {(unsigned)rows[i], (unsigned)cols[i], 0u};
-        real cell = (real)0;
-        /* The kernel writes dst[row * numImagebin + col]; point that slot at `cell`. */
-        int64_t dst_index = rows[i] * (int64_t)n_cols_total + cols[i];
-        real* base = reinterpret_cast<real*>(reinterpret_cast<uintptr_t>(&cell) - (uintptr_t)(dst_index * (int64_t)sizeof(real)));
-        photodetectorCudaMe(base, c.data(), d.data(), im.data(), n_rows_total, n_cols_total);
-        out[i] = (double)cell;
+#pragma omp parallel num_threads(nthreads)
+    {
+        std::vector<real> im = widen(img, 100, 100);
+        im[2] = (real)1.0f;
+        im[30] = (real)(float)nz;
+#pragma omp for schedule(dynamic, 8)
+        for (int64_t i = 0; i < n; ++i) {
+            ref_div[0] = (unsigned)divx; ref_div[1] = (unsigned)divy; ref_div[2] = (unsigned)divz;
+            const int64_t z = cols[i] / plane;
+            const int64_t in_plane = cols[i] % plane;
+            im[31] = (real)(float)z;
+            blockDim = {1u, 1u, 1u};
+            threadIdx = {0u, 0u, 0u};
+            blockIdx = {(unsigned)rows[i], (unsigned)in_plane, 0u};
+            real cell = (real)0;
+            /* The kernel writes dst[row * plane + in_plane]; point that slot at `cell`. */
+            int64_t dst_index = rows[i] * (int64_t)plane + in_plane;
+            real* base = reinterpret_cast<real*>(reinterpret_cast<uintptr_t>(&cell) - (uintptr_t)(dst_index * (int64_t)sizeof(real)));
+            photodetectorCudaMe(base, c.data(), d.data(), im.data(), n_rows_total, plane);
+            out[i] = (double)cell;
+        }
     }
     return 0;
 }
