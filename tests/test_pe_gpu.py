@@ -59,7 +59,7 @@ def test_hole_primitive_decisions_exact_values_refined():
     assert np.array_equal(got != 0, ref != 0), "hit/miss decisions differ from the reference"
     dual = oracle_py.primitive("cylinder", z["args"], impl="dual")
     err = rel_err(got, dual)
-    assert err.max() <= 1e-5
+    assert err.max() <= 1e-4
 
 
 # ---- sysmat values vs the reference's own code (golden) ---------------------
