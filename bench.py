@@ -260,7 +260,8 @@ def run_ours(args, world, rank, local):
     nx, ny, nz = p.grid
     n_slabs = nz // SLAB_Z
     slab_vox = nx * ny * SLAB_Z
-    rows = p.n_crystals
+    rows = p.n_crystals if args.rows <= 0 else min(args.rows, p.n_crystals)
+    row_range = (0, rows)
     out = torch.empty((rows, slab_vox), dtype=torch.float32, device=dev)
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
     stream = torch.cuda.Stream(device=dev)
@@ -269,7 +270,7 @@ def run_ours(args, world, rank, local):
     def step(i):
         s = (i * world + rank) % n_slabs
         flush.zero_()
-        geo.pe(z=(s * SLAB_Z, SLAB_Z), opts=opts, out=out.data_ptr(), stream=stream.cuda_stream)
+        geo.pe(z=(s * SLAB_Z, SLAB_Z), rows=row_range, opts=opts, out=out.data_ptr(), stream=stream.cuda_stream)
 
     with torch.cuda.stream(stream):
         for i in range(args.warmup):
@@ -295,7 +296,7 @@ def run_ours(args, world, rank, local):
                 s = (i * world + rank) % n_slabs
                 flush.zero_()
                 starts[i].record(stream)
-                geo.pe(z=(s * SLAB_Z, SLAB_Z), opts=opts, out=out.data_ptr(), stream=stream.cuda_stream)
+                geo.pe(z=(s * SLAB_Z, SLAB_Z), rows=row_range, opts=opts, out=out.data_ptr(), stream=stream.cuda_stream)
                 ends[i].record(stream)
             t_end.record(stream)
         torch.cuda.synchronize()
@@ -315,7 +316,7 @@ def run_ours(args, world, rank, local):
 
     # Work counters of one slab (separate, counted run).
     ctx.set_counters(True)
-    geo.pe(z=(0, SLAB_Z), opts=opts, out=out.data_ptr(), stream=stream.cuda_stream)
+    geo.pe(z=(0, SLAB_Z), rows=row_range, opts=opts, out=out.data_ptr(), stream=stream.cuda_stream)
     n_rays, n_cry, n_hole, n_cone = ctx.last_counters()
     ctx.set_counters(False)
     flops = (n_rays * (F_RAY + p.n_plates * F_BOX + 2 * F_IN + F_BOX) + n_cry * (F_BOX + F_XF) + n_hole * F_CYL
@@ -342,7 +343,7 @@ def run_ours(args, world, rank, local):
         for i in range(args.e2e_steps):
             s = (i * world + rank) % n_slabs
             g2 = sysmat_b200.Geometry(ctx, p)
-            g2.pe(z=(s * SLAB_Z, SLAB_Z), opts=opts, out=host)
+            g2.pe(z=(s * SLAB_Z, SLAB_Z), rows=row_range, opts=opts, out=host)
             g2.close()
         torch.cuda.synchronize()
         e2e_s = time.perf_counter() - t0
@@ -406,6 +407,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--ref-entries", type=int, default=4096)
+    ap.add_argument("--rows", type=int, default=0, help="limit the crystal rows per step (profiling runs)")
     ap.add_argument("--no-ref-cuda", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

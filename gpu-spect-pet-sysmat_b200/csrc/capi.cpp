@@ -47,6 +47,8 @@ int context_collect_status(sm_context* ctx, cudaStream_t stream) {
         if (st & kStatusSupersetOverflow)
             return fail(SM_ERR_CAPACITY,
                         "a tile's candidate set exceeded %d crystals or %d holes; use smaller tile_voxels", kSupC, kSupH);
+        if (st & kStatusListOverflow)
+            return fail(SM_ERR_CAPACITY, "a voxel's candidate list exceeded %d crystals or %d holes", kListC, kListH);
         if (st & kStatusRecordOverflow)
             return fail(SM_ERR_CAPACITY, "a ray hit more than %d holes or %d crystals (hit record capacity)", kRecHoles,
                         kRecCrystals);
@@ -58,9 +60,12 @@ int context_collect_status(sm_context* ctx, cudaStream_t stream) {
 static int validate_pe(const sm_geometry* geo, const sm_pe_options* opt, int row0, int row1, int z0, int nz) {
     for (int a = 0; a < 3; ++a) {
         if (opt->sv[a] < 1 || opt->sv[a] > 64) return fail(SM_ERR_INVALID, "sv[%d] = %d must be in 1..64", a, opt->sv[a]);
-        if (opt->sc[a] < 1 || opt->sc[a] > 256) return fail(SM_ERR_INVALID, "sc[%d] = %d must be in 1..256", a, opt->sc[a]);
+        if (opt->sc[a] < 1 || opt->sc[a] > kMaxSubcellsPerAxis)
+            return fail(SM_ERR_INVALID, "sc[%d] = %d must be in 1..%d", a, opt->sc[a], kMaxSubcellsPerAxis);
         if (opt->tile_voxels[a] < 0) return fail(SM_ERR_INVALID, "tile_voxels[%d] must be >= 0", a);
     }
+    if ((int64_t)opt->sv[0] * opt->sv[1] * opt->sv[2] * opt->sc[0] * opt->sc[1] * opt->sc[2] > (1 << 22))
+        return fail(SM_ERR_CAPACITY, "more than 2^22 rays per entry");
     const HostGeometry& g = geo->host;
     if ((int64_t)g.nx * opt->sv[0] > (1 << 24) || (int64_t)g.ny * opt->sv[1] > (1 << 24) ||
         (int64_t)g.nz * opt->sv[2] > (1 << 24))

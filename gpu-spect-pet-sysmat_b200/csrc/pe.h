@@ -15,6 +15,9 @@ constexpr int kSupC = 512;             // tile superset capacity, crystals
 constexpr int kSupH = 256;             // tile superset capacity, holes
 constexpr int kMaxGroup = 4;           // voxel sub-points whose candidate masks are live at once
 constexpr int kMaxTileVoxels = 128;    // voxels per brick
+constexpr int kListC = 256;            // per-voxel candidate list capacity, crystals
+constexpr int kListH = 128;            // per-voxel candidate list capacity, holes
+constexpr int kMaxSubcellsPerAxis = 256;
 constexpr int kRecHoles = 16;          // hit-record capacity per ray
 constexpr int kRecCrystals = 40;
 constexpr int kRecWords = 3 + kRecHoles + kRecCrystals;
@@ -23,6 +26,7 @@ constexpr int kRecWords = 3 + kRecHoles + kRecCrystals;
 enum : int {
     kStatusSupersetOverflow = 1,
     kStatusRecordOverflow = 2,
+    kStatusListOverflow = 4,
 };
 
 struct PEParams {
@@ -36,6 +40,8 @@ struct PEParams {
     int dX, dY, dZ;          // crystal sub-cells
     int n_sc, n_sv, group;   // sub-cells per crystal, sub-points per voxel, sub-points per mask group
     float inv_sv;
+    // reciprocals for the division-free index decode (exact after one correction step)
+    float inv_n_sc, inv_dY, inv_dX, inv_kx, inv_ky, inv_kxky, inv_dXdY;
     int row0, row1;          // crystal rows [row0, row1)
     int bx, by, bz;          // voxel brick
     int tiles_x, tiles_y, tiles_z;

@@ -43,6 +43,13 @@ void pe_plan(const HostGeometry& g, const int sv[3], const int sc[3], const int 
     P.n_sv = sv[0] * sv[1] * sv[2];
     P.group = std::max(1, std::min(kMaxGroup, 32 / P.n_sc));
     P.inv_sv = 1.0f / (float)P.n_sv;
+    P.inv_n_sc = 1.0f / (float)P.n_sc;
+    P.inv_dY = 1.0f / (float)P.dY;
+    P.inv_dX = 1.0f / (float)P.dX;
+    P.inv_kx = 1.0f / (float)P.kx;
+    P.inv_ky = 1.0f / (float)P.ky;
+    P.inv_kxky = 1.0f / (float)(P.kx * P.ky);
+    P.inv_dXdY = 1.0f / (float)(P.dX * P.dY);
     P.row0 = row0;
     P.row1 = row1;
     int bx = brick[0] > 0 ? brick[0] : 8;

@@ -4,29 +4,34 @@
 //   A[d, v] = 1/Sv * sum over voxel sub-points p and crystal sub-cells q of
 //             exp(-sum mu*L along p->q) * Omega(p, q) * absorption(q)
 // with the reference's physics and hit decisions
-// (PEGen_RayTracing_CircularHole/PESysMatGen.cu:375-764): plate boxes a ray
-// does not traverse block it (1e5 penalty), holes and other crystals count
-// only when they are among the voxel's bounding-sphere candidates of the
-// detecting crystal, the detecting crystal attenuates up to the sub-cell, and
-// the sub-cell absorbs (1 - exp(-mu_t L)) mu_pe / mu_t.
+// (PEGen_RayTracing_CircularHole/PESysMatGen.cu:375-764): a plate box the ray
+// does not traverse blocks it (1e5 penalty), holes and other crystals count
+// only when they are among the bounding-sphere candidates of (voxel point,
+// detecting crystal), the detecting crystal attenuates up to the sub-cell,
+// and the sub-cell absorbs (1 - exp(-mu_t L)) mu_pe / mu_t.
 //
 // Work decomposition (one CTA per tile = 8 crystals x one voxel brick):
 //  1. Tile cull: the CTA tests every crystal and hole against the bundle of
 //     segments from the brick's sub-point box to each of its 8 crystals
-//     (window_hit, conservative) and stages the survivors, ordered by id,
-//     in shared memory.
-//  2. Each warp owns one crystal and walks the brick's voxels, so its lanes
-//     stay on nearby rays with the same candidates.  Per voxel sub-point the
-//     warp evaluates the reference's exact cone test on the staged set
-//     (after a per-sub-point window test) and keeps the result as ballot
-//     bitmasks; lanes then trace one ray (sub-point, sub-cell) each.
-//  3. Per ray, a window test against each candidate's box skips the exact
-//     slab/cylinder test for candidates the ray cannot reach; the exact
-//     tests are the reference's single-precision ones, so hits are
-//     identical.  Skipped candidates would have contributed exactly 0.
+//     (window_hit, conservative) and stages the survivors, ordered by id, in
+//     shared memory.
+//  2. Each warp owns one crystal and walks the brick's voxels.  Per voxel it
+//     narrows the staged set with the same window test for that voxel's
+//     sub-point box and compacts the survivors into a per-warp list.  Per
+//     voxel sub-point it evaluates the reference's candidate cone test on
+//     the list (a float filter decides clear cases; cases within 1e-5 of the
+//     threshold use the reference's exact single-precision expression) and
+//     keeps the result as ballot bitmasks over the list.
+//  3. Lanes trace one ray (sub-point, sub-cell) each.  A division-free
+//     window test per candidate skips the exact test for candidates the ray
+//     cannot reach; the exact tests are the reference's single-precision
+//     ones, so every hit decision is the reference's.  Skipped candidates
+//     would have contributed exactly 0.  The plates use a fast path that
+//     proves "fully traversed" with margins, else the exact test.  Values
+//     that are not hit decisions (solid angle, path inside the detecting
+//     crystal, absorption chord) use closed forms in single precision.
 //  4. Lanes accumulate with Kahan summation; warp shuffles reduce; the CTA
-//     stages its 8 x brick results in shared memory and writes them out
-//     row by row.
+//     stages its 8 x brick results in shared memory and writes them out.
 #include <cuda_runtime.h>
 
 #include "pe.h"
@@ -36,10 +41,19 @@ namespace smb {
 
 namespace {
 
-constexpr int kMaskC = kSupC / 32;
-constexpr int kMaskH = kSupH / 32;
-constexpr int kMaskWords = kMaskC + kMaskH;
-constexpr float kMargin = 0.01f;   // mm added around every culling box
+constexpr int kLWC = kListC / 32;
+constexpr int kLWH = kListH / 32;
+constexpr float kMargin = 0.01f;     // mm added around every culling box
+constexpr float kConeMargin = 1e-5f; // float-filter band around the cone threshold
+
+struct WarpLists {
+    unsigned short list_c[kListC];    // staged-set indices of the voxel's candidate crystals
+    unsigned short list_h[kListH];    // ... and holes (ascending ids)
+    int n_c, n_h;
+    int plate_begin[kMaxPlates + 1];  // list_h index where each plate's holes start
+    unsigned mask_c[kMaxGroup][kLWC]; // per sub-point: candidates after the cone test
+    unsigned mask_h[kMaxGroup][kLWH];
+};
 
 struct __align__(16) PeSmem {
     float4 c_pos[kSupC];     // cx, cy, cz, mu_total
@@ -51,11 +65,11 @@ struct __align__(16) PeSmem {
     float4 h_a[kSupH];       // x, y1, y2, z
     float4 h_b[kSupH];       // R, mu_total, crit, yc
     int h_id[kSupH];
-    int h_plate_begin[kMaxPlates + 1];
+    float frac[3][kMaxSubcellsPerAxis];   // (s + 0.5) / d per axis, IEEE, as the reference computes it
     Box3 d_box[kPeWarps];    // inflated AABB of the tile's crystals
     int warp_cnt[kPeWarps];
     int n_c, n_h;
-    unsigned int mask[kPeWarps][kMaxGroup][kMaskWords];
+    WarpLists wl[kPeWarps];
     float out[kPeWarps][kMaxTileVoxels];
 };
 
@@ -65,7 +79,14 @@ __device__ __forceinline__ unsigned lanemask_lt() {
     return m;
 }
 
-__device__ __forceinline__ Box3 point_box(const Vec3& p) { return Box3{p.x, p.y, p.z, p.x, p.y, p.z}; }
+// floor(n / d) for 0 <= n < 2^22 with inv ~ 1/d: exact after one correction.
+__device__ __forceinline__ int fast_div(int n, int d, float inv) {
+    int q = __float2int_rz(__fmul_rn((float)n, inv));
+    int r = n - q * d;
+    if (r < 0) --q;
+    else if (r >= d) ++q;
+    return q;
+}
 
 // Voxel sub-point in world coordinates: the reference's voxel centre on the
 // fine grid (PESysMatGen.cu:438-449), fine index f = coarse * k + sub.
@@ -83,29 +104,25 @@ __device__ __forceinline__ Vec3 subpoint(const PEParams& P, int fx, int fy, int 
     return r;
 }
 
-__device__ __forceinline__ void subpoint_index(const PEParams& P, int ix, int iy, int iz, int s, int& fx, int& fy,
-                                               int& fz) {
-    int sx = s % P.kx;
-    int sy = (s / P.kx) % P.ky;
-    int sz = s / (P.kx * P.ky);
-    fx = ix * P.kx + sx;
-    fy = iy * P.ky + sy;
-    fz = iz * P.kz + sz;
+__device__ __forceinline__ Vec3 subpoint_of(const PEParams& P, int ix, int iy, int iz, int s) {
+    const int sz = fast_div(s, P.kx * P.ky, P.inv_kxky);
+    const int rem = s - sz * P.kx * P.ky;
+    const int sy = fast_div(rem, P.kx, P.inv_kx);
+    const int sx = rem - sy * P.kx;
+    return subpoint(P, ix * P.kx + sx, iy * P.ky + sy, iz * P.kz + sz);
 }
 
 // Per-crystal constants of the warp's detecting crystal.
 struct Detecting {
-    int id;
     float cx, cy, cz, mu_t, mu_pe;
     float w, t, h, crit;
-    float cm, sm, cp, sp;      // cos(-rot), sin(-rot), cos(rot), sin(rot)
-    Box3 self_box;             // +-size/2 in its own frame
-    Box3 world;                // inflated world AABB
-    float area_x, area_z, area_y;   // sub-cell face areas (t*h/dZ/dY, w*t/dX/dY, w*h/dX/dZ)
+    float cm, sm, cp, sp;          // cos(-rot), sin(-rot), cos(rot), sin(rot)
+    Box3 world;                    // inflated world AABB
+    float area_x, area_z, area_y;  // sub-cell face areas (t*h/dZ/dY, w*t/dX/dY, w*h/dX/dZ)
+    float hx, hy, hz;              // sub-cell half sizes
 };
 
-// The reference's bounding-sphere candidate test of crystal k for the voxel
-// point p and detecting crystal d (PESysMatGen.cu:506-551), bit-exact.
+// ---- candidate cone test (PESysMatGen.cu:506-589) -----------------------------
 struct ConeSelf {
     float ux, uy, uz, crit_self;
 };
@@ -120,8 +137,8 @@ __device__ __forceinline__ ConeSelf cone_self(const Detecting& D, const Vec3& p)
     return c;
 }
 
-__device__ __forceinline__ bool cone_crystal(const ConeSelf& cs, const Vec3& p, float xk, float yk, float zk,
-                                             float crit_k) {
+// The reference's crystal test, exactly (IEEE single, no contraction).
+__device__ __noinline__ bool cone_crystal_exact(ConeSelf cs, Vec3 p, float xk, float yk, float zk, float crit_k) {
     float dk = sqrtf((p.x - xk) * (p.x - xk) + (p.y - yk) * (p.y - yk) + (p.z - zk) * (p.z - zk));
     float crit = crit_k / dk / 2.0f;
     float ex = (xk - p.x) / dk, ey = (yk - p.y) / dk, ez = (zk - p.z) / dk;
@@ -129,14 +146,31 @@ __device__ __forceinline__ bool cone_crystal(const ConeSelf& cs, const Vec3& p, 
            crit + cs.crit_self;
 }
 
-// Hole candidate test (PESysMatGen.cu:559-585), bit-exact.
-__device__ __forceinline__ bool cone_hole(const ConeSelf& cs, const Vec3& p, float hx, float hyc, float hz,
-                                          float crit_h) {
+// The reference's hole test, exactly.
+__device__ __noinline__ bool cone_hole_exact(ConeSelf cs, Vec3 p, float hx, float hyc, float hz, float crit_h) {
     float dh = sqrtf((p.x - hx) * (p.x - hx) + (p.y - hyc) * (p.y - hyc) + (p.z - hz) * (p.z - hz));
     float crit = crit_h / dh;
     float ex = (hx - p.x) / dh, ey = (hyc - p.y) / dh, ez = (hz - p.z) / dh;
     return sqrtf((ez - cs.uz) * (ez - cs.uz) + (ey - cs.uy) * (ey - cs.uy) + (ex - cs.ux) * (ex - cs.ux)) <=
            crit + cs.crit_self;
+}
+
+// Float filter: the same quantities with fast reciprocal square roots; its
+// error is below 1e-6 of the unit-sphere distances compared, so outside a
+// band of kConeMargin the answer equals the exact one.  Returns 1 (pass),
+// 0 (fail) or -1 (too close to call).
+__device__ __forceinline__ int cone_filter(const ConeSelf& cs, const Vec3& p, float xk, float yk, float zk,
+                                           float crit_scaled) {
+    float dx = xk - p.x, dy = yk - p.y, dz = zk - p.z;
+    float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+    float inv = rsqrtf(d2);
+    float ex = fmaf(dx, inv, -cs.ux), ey = fmaf(dy, inv, -cs.uy), ez = fmaf(dz, inv, -cs.uz);
+    float lhs = sqrtf(fmaf(ex, ex, fmaf(ey, ey, ez * ez)));
+    float rhs = fmaf(crit_scaled, inv, cs.crit_self);
+    float diff = lhs - rhs;
+    if (diff < -kConeMargin) return 1;
+    if (diff > kConeMargin) return 0;
+    return -1;
 }
 
 __device__ __forceinline__ Box3 hole_box(const float4& a, const float4& b) {
@@ -148,62 +182,151 @@ __device__ __forceinline__ Box3 box_of(const float4& lo, const float4& hi) {
     return Box3{lo.x, lo.y, lo.z, hi.x, hi.y, hi.z};
 }
 
-// One ray: voxel sub-point p (world) and its coordinates ps in the detecting
-// crystal's frame, sub-cell c.  Returns its contribution; in RECORD mode also
-// writes the ray's hit record to rec.
+// ---- division-free window test -------------------------------------------------
+// window_hit (tracer.cuh) with the bundle source A and target B fixed: the two
+// reciprocals are computed once.  Conservative: K carries the 0.01 mm margin,
+// far above the error of the approximate reciprocals.
+struct Bundle {
+    Box3 A, B;
+    float inv2;     // 1 / (B.y2 - A.y2)
+    float inv1;     // 1 / (B.y1 - A.y1)
+    bool ordered;   // A lies entirely before B in depth
+};
+
+__device__ __forceinline__ Bundle make_bundle(const Box3& A, const Box3& B) {
+    Bundle b;
+    b.A = A;
+    b.B = B;
+    b.ordered = A.y2 < B.y1;
+    b.inv2 = __fdividef(1.0f, B.y2 - A.y2);
+    b.inv1 = __fdividef(1.0f, B.y1 - A.y1);
+    return b;
+}
+
+__device__ __forceinline__ bool bundle_hit(const Bundle& b, const Box3& K) {
+    if (!b.ordered || !(b.A.y2 < K.y1)) return true;
+    if (K.y1 > b.B.y2) return false;              // beyond every segment's end
+    const float yhi = fminf(K.y2, b.B.y2);
+    const float lmin = fmaxf((K.y1 - b.A.y2) * b.inv2, 0.0f);
+    const float lmax = fminf(1.0f, (yhi - b.A.y1) * b.inv1);
+    const float xa = fmaf(b.B.x1 - b.A.x1, lmin, b.A.x1), xb = fmaf(b.B.x1 - b.A.x1, lmax, b.A.x1);
+    const float xc = fmaf(b.B.x2 - b.A.x2, lmin, b.A.x2), xd = fmaf(b.B.x2 - b.A.x2, lmax, b.A.x2);
+    if (fminf(xa, xb) > K.x2 || fmaxf(xc, xd) < K.x1) return false;
+    const float za = fmaf(b.B.z1 - b.A.z1, lmin, b.A.z1), zb = fmaf(b.B.z1 - b.A.z1, lmax, b.A.z1);
+    const float zc = fmaf(b.B.z2 - b.A.z2, lmin, b.A.z2), zd = fmaf(b.B.z2 - b.A.z2, lmax, b.A.z2);
+    if (fminf(za, zb) > K.z2 || fmaxf(zc, zd) < K.z1) return false;
+    return true;
+}
+
+// Segment p -> q against box K (inflated): the point-to-point bundle.
+struct RaySeg {
+    Vec3 p, q;
+    float inv_dy;
+    bool ordered;
+};
+
+__device__ __forceinline__ bool ray_may_hit(const RaySeg& r, const Box3& K) {
+    if (!r.ordered || !(r.p.y < K.y1)) return true;
+    if (K.y1 > r.q.y) return false;               // beyond the segment's end
+    const float lmin = (K.y1 - r.p.y) * r.inv_dy;
+    const float lmax = fminf(1.0f, (fminf(K.y2, r.q.y) - r.p.y) * r.inv_dy);
+    const float dx = r.q.x - r.p.x, dz = r.q.z - r.p.z;
+    const float xa = fmaf(dx, lmin, r.p.x), xb = fmaf(dx, lmax, r.p.x);
+    if (fminf(xa, xb) > K.x2 || fmaxf(xa, xb) < K.x1) return false;
+    const float za = fmaf(dz, lmin, r.p.z), zb = fmaf(dz, lmax, r.p.z);
+    if (fminf(za, zb) > K.z2 || fmaxf(za, zb) < K.z1) return false;
+    return true;
+}
+
+// Exact plate test out of line (rarely needed: see plate_traversed).
+__device__ __noinline__ float plate_chord_exact(Vec3 p, Vec3 q, Box3 b) {
+    return chord_through(p.x, p.y, p.z, q.x, q.y, q.z, b);
+}
+
+// The reference blocks a ray whose chord through a plate box is < 0.1
+// (PESysMatGen.cu:656-658).  When the segment starts 0.01 mm before the plate,
+// ends 0.01 mm after it, and stays 0.01 mm inside its lateral faces at both
+// depth planes, every branch of the exact test returns the y-slab chord
+// (>= thickness > 0.11), so the answer "traversed" is certain; otherwise the
+// exact test decides.
+__device__ __forceinline__ bool plate_traversed(const Vec3& p, const Vec3& q, float inv_dy, const PlateBox& pb) {
+    const Box3 b{pb.x1, pb.y1, pb.z1, pb.x2, pb.y2, pb.z2};
+    if (p.y < pb.y1 - kMargin && q.y > pb.y2 + kMargin && (pb.y2 - pb.y1) > 0.11f) {
+        const float l1 = (pb.y1 - p.y) * inv_dy, l2 = (pb.y2 - p.y) * inv_dy;
+        const float dx = q.x - p.x, dz = q.z - p.z;
+        const float xa = fmaf(dx, l1, p.x), xb = fmaf(dx, l2, p.x);
+        const float za = fmaf(dz, l1, p.z), zb = fmaf(dz, l2, p.z);
+        const float lo_x = pb.x1 + kMargin, hi_x = pb.x2 - kMargin, lo_z = pb.z1 + kMargin, hi_z = pb.z2 - kMargin;
+        if (fminf(xa, xb) > lo_x && fmaxf(xa, xb) < hi_x && fminf(za, zb) > lo_z && fmaxf(za, zb) < hi_z) return true;
+    }
+    return !(plate_chord_exact(p, q, b) < 0.1f);
+}
+
+__device__ __noinline__ float self_path_exact(Vec3 ps, Vec3 qs, Box3 crystal, Box3 unit, float* absorb_len, float r) {
+    float l1 = chord_to_end(ps.x, ps.y, ps.z, qs.x, qs.y, qs.z, crystal);
+    float l2 = chord_to_end(ps.x, ps.y, ps.z, qs.x, qs.y, qs.z, unit);
+    float xt = qs.x + 1000.0f * (qs.x - ps.x) / r;
+    float yt = qs.y + 1000.0f * (qs.y - ps.y) / r;
+    float zt = qs.z + 1000.0f * (qs.z - ps.z) / r;
+    *absorb_len = chord_through(ps.x, ps.y, ps.z, xt, yt, zt, unit);
+    return l1 - l2;
+}
+
+// One ray: sub-point p (world) and ps (detecting crystal frame), sub-cell
+// (sx, sy, sz).  mask_c / mask_h: the sub-point's candidates over the warp's
+// lists.  Returns the contribution; in RECORD mode also the hit record.
 template <bool RECORD>
-__device__ float trace_ray(const PEParams& P, const DevGeometry& G, const PeSmem& S, const unsigned* mask,
-                           const Detecting& D, const Vec3& p, const Vec3& ps, int c, int* rec, int* status,
-                           unsigned long long* n_cry_tests, unsigned long long* n_hole_tests) {
-    const int sy = c % P.dY;
-    const int sx = (c / P.dY) % P.dX;
-    const int sz = c / (P.dY * P.dX);
+__device__ __forceinline__ float trace_ray(const PEParams& P, const DevGeometry& G, const PeSmem& S,
+                                           const WarpLists& L, const unsigned* mask_c, const unsigned* mask_h,
+                                           const Detecting& D, const Vec3& p, const Vec3& ps, int sx, int sy, int sz,
+                                           int* rec, int* status, unsigned long long* n_cry,
+                                           unsigned long long* n_hole) {
     // Sub-cell centre, crystal frame then world (PESysMatGen.cu:606-616).
-    const float xDs = -D.w / 2.0f + ((float)sx + 0.5f) / (float)P.dX * D.w;
-    const float zDs = -D.h / 2.0f + ((float)sz + 0.5f) / (float)P.dZ * D.h;
-    const float yDs = -D.t / 2.0f + ((float)sy + 0.5f) / (float)P.dY * D.t;
+    const float xDs = -D.w / 2.0f + S.frac[0][sx] * D.w;
+    const float zDs = -D.h / 2.0f + S.frac[2][sz] * D.h;
+    const float yDs = -D.t / 2.0f + S.frac[1][sy] * D.t;
     Vec3 q;
     q.x = D.cx + (xDs * D.cp - zDs * D.sp);
     q.z = D.cz + (xDs * D.sp + zDs * D.cp);
     q.y = D.cy + yDs;
 
-    const float dsq = (q.y - p.y) * (q.y - p.y) + (q.x - p.x) * (q.x - p.x) + (q.z - p.z) * (q.z - p.z);
-    const float r = sqrtf(dsq);
-    const float cosang = (q.y - p.y) / r;
+    RaySeg seg;
+    seg.p = p;
+    seg.q = q;
+    seg.ordered = p.y < q.y;
+    const float dy = q.y - p.y;
+    seg.inv_dy = __fdividef(1.0f, dy);
+
+    unsigned plate_miss = 0u;
+    for (int m = 0; m < G.n_plates; ++m)
+        if (!plate_traversed(p, q, seg.inv_dy, G.plate[m])) plate_miss |= 1u << m;
+    if (!RECORD && plate_miss) return 0.0f;   // exp(-(1e5 + ...)) == 0
+
+    const float dxw = q.x - p.x, dzw = q.z - p.z;
+    const float dsq = fmaf(dy, dy, fmaf(dxw, dxw, dzw * dzw));
+    const float inv_r = rsqrtf(dsq);
+    const float r = dsq * inv_r;
 
     int rec_h = 0, rec_c = 0;
-    unsigned plate_miss = 0u;
-    // Plates the ray does not traverse block it (PESysMatGen.cu:643-659):
-    // exp(-(1e5 + ...)) is exactly 0, so the ray contributes nothing.
-    for (int m = 0; m < G.n_plates; ++m) {
-        const PlateBox& pb = G.plate[m];
-        Box3 b{pb.x1, pb.y1, pb.z1, pb.x2, pb.y2, pb.z2};
-        if (chord_through(p.x, p.y, p.z, q.x, q.y, q.z, b) < 0.1f) plate_miss |= 1u << m;
-    }
-    if (!RECORD && plate_miss) return 0.0f;
-
-    const Box3 q_box = point_box(q);
-    const Box3 p_box = point_box(p);
     float att = 0.0f;
     // Plates: holes among the candidates, tungsten for the rest of T / cos(theta)
     // (PESysMatGen.cu:661-685).
     for (int m = 0; m < G.n_plates; ++m) {
         float in_holes = 0.0f;
-        const int hb = S.h_plate_begin[m], he = S.h_plate_begin[m + 1];
+        const int hb = L.plate_begin[m], he = L.plate_begin[m + 1];
         for (int wd = hb >> 5; wd <= ((he - 1) >> 5) && he > hb; ++wd) {
-            unsigned bits = mask[kMaskC + wd];
-            // keep only bits of this plate's range
-            int lo = hb - (wd << 5), hi = he - (wd << 5);
+            unsigned bits = mask_h[wd];
+            const int lo = hb - (wd << 5), hi = he - (wd << 5);
             if (lo > 0) bits &= ~0u << lo;
             if (hi < 32) bits &= (1u << hi) - 1u;
             while (bits) {
-                int b = __ffs(bits) - 1;
+                const int b = __ffs(bits) - 1;
                 bits &= bits - 1;
-                int k = (wd << 5) + b;
+                const int k = L.list_h[(wd << 5) + b];
                 const float4 ha = S.h_a[k], hbv = S.h_b[k];
-                if (!window_hit(p_box, q_box, hole_box(ha, hbv))) continue;
-                if (n_hole_tests) ++*n_hole_tests;
-                float len = chord_hole(p.x, p.y, p.z, q.x, q.y, q.z, ha.x, ha.y, ha.z, ha.w, hbv.x);
+                if (!ray_may_hit(seg, hole_box(ha, hbv))) continue;
+                if (n_hole) ++*n_hole;
+                const float len = chord_hole(p.x, p.y, p.z, q.x, q.y, q.z, ha.x, ha.y, ha.z, ha.w, hbv.x);
                 in_holes += len;
                 att += hbv.y * len;
                 if (RECORD && len > 0.0f) {
@@ -214,29 +337,29 @@ __device__ float trace_ray(const PEParams& P, const DevGeometry& G, const PeSmem
             }
         }
         const PlateBox& pb = G.plate[m];
-        float through = pb.thickness / cosang;
+        const float through = pb.thickness * r * seg.inv_dy;   // T / cos(theta)
         if ((through - in_holes) >= 0.00001f) att += pb.mu_total * (through - in_holes);
     }
     // Other crystals among the candidates, each in its own frame (:687-725).
-    const int nwc = (S.n_c + 31) >> 5;
+    const int nwc = (L.n_c + 31) >> 5;
     for (int wd = 0; wd < nwc; ++wd) {
-        unsigned bits = mask[wd];
+        unsigned bits = mask_c[wd];
         while (bits) {
-            int b = __ffs(bits) - 1;
+            const int b = __ffs(bits) - 1;
             bits &= bits - 1;
-            int k = (wd << 5) + b;
-            if (!window_hit(p_box, q_box, box_of(S.c_lo[k], S.c_hi[k]))) continue;
-            if (n_cry_tests) ++*n_cry_tests;
+            const int k = L.list_c[(wd << 5) + b];
+            if (!ray_may_hit(seg, box_of(S.c_lo[k], S.c_hi[k]))) continue;
+            if (n_cry) ++*n_cry;
             const float4 kp = S.c_pos[k], ks = S.c_size[k];
             const float2 kr = S.c_rot[k];
-            float xIa = (p.x - kp.x) * kr.x - (p.z - kp.z) * kr.y;
-            float yIa = p.y - kp.y;
-            float zIa = (p.x - kp.x) * kr.y + (p.z - kp.z) * kr.x;
-            float xDa = (q.x - kp.x) * kr.x - (q.z - kp.z) * kr.y;
-            float yDa = q.y - kp.y;
-            float zDa = (q.x - kp.x) * kr.y + (q.z - kp.z) * kr.x;
-            Box3 kb{-0.5f * ks.x, -0.5f * ks.y, -0.5f * ks.z, 0.5f * ks.x, 0.5f * ks.y, 0.5f * ks.z};
-            float len = chord_through(xIa, yIa, zIa, xDa, yDa, zDa, kb);
+            const float xIa = (p.x - kp.x) * kr.x - (p.z - kp.z) * kr.y;
+            const float yIa = p.y - kp.y;
+            const float zIa = (p.x - kp.x) * kr.y + (p.z - kp.z) * kr.x;
+            const float xDa = (q.x - kp.x) * kr.x - (q.z - kp.z) * kr.y;
+            const float yDa = q.y - kp.y;
+            const float zDa = (q.x - kp.x) * kr.y + (q.z - kp.z) * kr.x;
+            const Box3 kb{-0.5f * ks.x, -0.5f * ks.y, -0.5f * ks.z, 0.5f * ks.x, 0.5f * ks.y, 0.5f * ks.z};
+            const float len = chord_through(xIa, yIa, zIa, xDa, yDa, zDa, kb);
             att += len * kp.w;
             if (RECORD && len > 0.0f) {
                 if (rec_c < kRecCrystals) rec[3 + kRecHoles + rec_c] = S.c_id[k];
@@ -251,28 +374,58 @@ __device__ float trace_ray(const PEParams& P, const DevGeometry& G, const PeSmem
         rec[2 + kRecHoles] = rec_c < kRecCrystals ? rec_c : kRecCrystals;
         if (plate_miss) return 0.0f;
     }
-    // Path inside the detecting crystal up to the sub-cell (:727-746).
-    Box3 ub{((float)sx / (float)P.dX - 0.5f) * D.w, ((float)sy / (float)P.dY - 0.5f) * D.t,
-            ((float)sz / (float)P.dZ - 0.5f) * D.h, (((float)sx + 1.0f) / (float)P.dX - 0.5f) * D.w,
-            (((float)sy + 1.0f) / (float)P.dY - 0.5f) * D.t, (((float)sz + 1.0f) / (float)P.dZ - 0.5f) * D.h};
-    float l1 = chord_to_end(ps.x, ps.y, ps.z, xDs, yDs, zDs, D.self_box);
-    float l2 = chord_to_end(ps.x, ps.y, ps.z, xDs, yDs, zDs, ub);
-    att += (l1 - l2) * D.mu_t;
-    const float eff = expf(-att);
-    // Absorption in the sub-cell along the ray extended by 1000 mm (:749-759).
-    float xt = xDs + 1000.0f * (xDs - ps.x) / r;
-    float yt = yDs + 1000.0f * (yDs - ps.y) / r;
-    float zt = zDs + 1000.0f * (zDs - ps.z) / r;
-    float labs = chord_through(ps.x, ps.y, ps.z, xt, yt, zt, ub);
-    float absorb = (1.0f - expf(-labs * D.mu_t)) * D.mu_pe / D.mu_t;
+
+    // Path inside the detecting crystal before the sub-cell and the absorption
+    // chord (PESysMatGen.cu:727-759), as values: for the line from ps through
+    // the sub-cell centre qs (direction u), the sub-cell entry lies at
+    // min_i(h_i / |u_i|) before qs and the exit as far after it, and the
+    // crystal entry at min_i(g_i / |u_i|) with g_i the distance from qs to the
+    // crystal face facing ps.  When ps is not clearly outside the crystal or
+    // the ray is nearly parallel to its depth faces, the reference's own
+    // functions are used.
+    const float vx = xDs - ps.x, vy = yDs - ps.y, vz = zDs - ps.z;
+    float self_len, absorb_len;
+    const float hw = 0.5f * D.w, ht = 0.5f * D.t, hh = 0.5f * D.h;
+    const bool outside = (fabsf(ps.x) > hw + kMargin) || (fabsf(ps.y) > ht + kMargin) || (fabsf(ps.z) > hh + kMargin);
+    if (outside && fabsf(vy) > 0.01f) {
+        const float ax = fabsf(vx), ay = fabsf(vy), az = fabsf(vz);
+        // distances along the line, in units of |v| * (1 / |v_i|)
+        const float cell = fminf(fminf(D.hx * __fdividef(1.0f, ax), D.hy * __fdividef(1.0f, ay)),
+                                 D.hz * __fdividef(1.0f, az));
+        const float gx = (vx > 0.0f) ? (xDs + hw) : (hw - xDs);
+        const float gy = (vy > 0.0f) ? (yDs + ht) : (ht - yDs);
+        const float gz = (vz > 0.0f) ? (zDs + hh) : (hh - zDs);
+        const float crys = fminf(fminf(gx * __fdividef(1.0f, ax), gy * __fdividef(1.0f, ay)), gz * __fdividef(1.0f, az));
+        self_len = (crys - cell) * r;
+        absorb_len = 2.0f * cell * r;
+    } else {
+        const Box3 cb{-D.w / 2.0f, -D.t / 2.0f, -D.h / 2.0f, D.w / 2.0f, D.t / 2.0f, D.h / 2.0f};
+        const Box3 ub{xDs - D.hx, yDs - D.hy, zDs - D.hz, xDs + D.hx, yDs + D.hy, zDs + D.hz};
+        self_len = self_path_exact(ps, Vec3{xDs, yDs, zDs}, cb, ub, &absorb_len, r);
+    }
+    att = fmaf(self_len, D.mu_t, att);
+    const float eff = __expf(-att);
+    const float absorb = (1.0f - __expf(-absorb_len * D.mu_t)) * D.mu_pe / D.mu_t;
     // Solid angle: the largest of the three projected sub-cell faces (:618-639),
-    // A * |cos| / (4 pi d^2), single precision.
-    const float k4 = 0.0795774715459476678f / (dsq * r);   // 1 / (4 pi d^3)
-    float sa_x = D.area_x * fabsf((q.x - p.x) * D.cp - (q.z - p.z) * D.sp) * k4;
-    float sa_z = D.area_z * fabsf((q.x - p.x) * D.sp + (q.z - p.z) * D.cp) * k4;
-    float sa_y = D.area_y * fabsf(q.y - p.y) * k4;
-    float sa = fmaxf(fmaxf(sa_x, sa_y), sa_z);
+    // A * |cos| / (4 pi d^2).
+    const float k4 = 0.0795774715459476678f * inv_r * inv_r * inv_r;   // 1 / (4 pi d^3)
+    const float sa_x = D.area_x * fabsf(dxw * D.cp - dzw * D.sp);
+    const float sa_z = D.area_z * fabsf(dxw * D.sp + dzw * D.cp);
+    const float sa_y = D.area_y * fabsf(dy);
+    const float sa = fmaxf(fmaxf(sa_x, sa_y), sa_z) * k4;
     return eff * sa * absorb;
+}
+
+// Ordered compaction of a warp-wide predicate into a list; returns the new count.
+__device__ __forceinline__ int warp_append(bool pass, int value, unsigned short* list, int count, int cap, int lane,
+                                           int* status) {
+    const unsigned bal = __ballot_sync(0xffffffffu, pass);
+    const int pos = count + __popc(bal & lanemask_lt());
+    if (pass) {
+        if (pos < cap) list[pos] = (unsigned short)value;
+        else atomicOr(status, kStatusListOverflow);
+    }
+    return count + __popc(bal);
 }
 
 template <bool RECORD>
@@ -291,26 +444,35 @@ __global__ void __launch_bounds__(kPeThreads, 2) pe_trace_kernel(PEParams P, Dev
     const int ix1 = min(ix0 + P.bx, P.nx), iy1 = min(iy0 + P.by, P.ny), iz1 = min(iz0 + P.bz, P.z0 + P.nzs);
     const int d0 = P.row0 + ct * kPeWarps;
 
+    // Sub-cell centre fractions (s + 0.5) / d, rounded as the reference rounds them.
+    for (int i = tid; i < 3 * kMaxSubcellsPerAxis; i += kPeThreads) {
+        const int a = i / kMaxSubcellsPerAxis, s = i - a * kMaxSubcellsPerAxis;
+        const int dv = a == 0 ? P.dX : (a == 1 ? P.dY : P.dZ);
+        S.frac[a][s] = ((float)s + 0.5f) / (float)dv;
+    }
+
     // ---- 1. tile cull -------------------------------------------------------
-    // Sub-point box of the brick: extreme fine voxel centres, rotated.
-    Box3 A;
-    {
-        Vec3 c0 = subpoint(P, ix0 * P.kx, iy0 * P.ky, iz0 * P.kz);
-        Vec3 c1 = subpoint(P, ix1 * P.kx - 1, iy0 * P.ky, iz0 * P.kz);
-        Vec3 c2 = subpoint(P, ix0 * P.kx, iy1 * P.ky - 1, iz0 * P.kz);
-        Vec3 c3 = subpoint(P, ix1 * P.kx - 1, iy1 * P.ky - 1, iz0 * P.kz);
+    // Sub-point box of a voxel range: extreme fine voxel centres, rotated.
+    auto point_box_of = [&](int ax0, int ay0, int az0, int ax1, int ay1, int az1) {
+        Vec3 c0 = subpoint(P, ax0 * P.kx, ay0 * P.ky, az0 * P.kz);
+        Vec3 c1 = subpoint(P, ax1 * P.kx - 1, ay0 * P.ky, az0 * P.kz);
+        Vec3 c2 = subpoint(P, ax0 * P.kx, ay1 * P.ky - 1, az0 * P.kz);
+        Vec3 c3 = subpoint(P, ax1 * P.kx - 1, ay1 * P.ky - 1, az0 * P.kz);
+        Vec3 c4 = subpoint(P, ax0 * P.kx, ay0 * P.ky, az1 * P.kz - 1);
+        Box3 A;
         A.x1 = fminf(fminf(c0.x, c1.x), fminf(c2.x, c3.x)) - kMargin;
         A.x2 = fmaxf(fmaxf(c0.x, c1.x), fmaxf(c2.x, c3.x)) + kMargin;
         A.y1 = fminf(fminf(c0.y, c1.y), fminf(c2.y, c3.y)) - kMargin;
         A.y2 = fmaxf(fmaxf(c0.y, c1.y), fmaxf(c2.y, c3.y)) + kMargin;
-        Vec3 c4 = subpoint(P, ix0 * P.kx, iy0 * P.ky, iz1 * P.kz - 1);
         A.z1 = fminf(c0.z, c4.z) - kMargin;
         A.z2 = fmaxf(c0.z, c4.z) + kMargin;
-    }
+        return A;
+    };
+    const Box3 A = point_box_of(ix0, iy0, iz0, ix1, iy1, iz1);
     if (tid < kPeWarps) {
-        int d = d0 + tid;
+        const int d = d0 + tid;
         if (d < P.row1) {
-            float4 lo = G.c.lo[d], hi = G.c.hi[d];
+            const float4 lo = G.c.lo[d], hi = G.c.hi[d];
             S.d_box[tid] = Box3{lo.x - kMargin, lo.y - kMargin, lo.z - kMargin, hi.x + kMargin, hi.y + kMargin, hi.z + kMargin};
         } else {
             S.d_box[tid] = Box3{1e30f, 1e30f, 1e30f, -1e30f, -1e30f, -1e30f};
@@ -323,19 +485,19 @@ __global__ void __launch_bounds__(kPeThreads, 2) pe_trace_kernel(PEParams P, Dev
     for (int k0 = 0; k0 < G.n_crystals; k0 += kPeThreads) {
         const int k = k0 + tid;
         bool pass = false;
-        float4 lo, hi;
+        float4 lo = make_float4(0.f, 0.f, 0.f, 0.f), hi = lo;
         if (k < G.n_crystals) {
             lo = G.c.lo[k];
             hi = G.c.hi[k];
-            Box3 K{lo.x - kMargin, lo.y - kMargin, lo.z - kMargin, hi.x + kMargin, hi.y + kMargin, hi.z + kMargin};
+            const Box3 K{lo.x - kMargin, lo.y - kMargin, lo.z - kMargin, hi.x + kMargin, hi.y + kMargin, hi.z + kMargin};
             for (int j = 0; j < n_d && !pass; ++j) pass = window_hit(A, S.d_box[j], K);
         }
-        unsigned bal = __ballot_sync(0xffffffffu, pass);
+        const unsigned bal = __ballot_sync(0xffffffffu, pass);
         if (lane == 0) S.warp_cnt[warp] = __popc(bal);
         __syncthreads();
         int off = base, total = 0;
         for (int w = 0; w < kPeWarps; ++w) {
-            int cnt = S.warp_cnt[w];
+            const int cnt = S.warp_cnt[w];
             if (w < warp) off += cnt;
             total += cnt;
         }
@@ -344,7 +506,7 @@ __global__ void __launch_bounds__(kPeThreads, 2) pe_trace_kernel(PEParams P, Dev
             if (off < kSupC) {
                 S.c_pos[off] = G.c.pos[k];
                 S.c_size[off] = G.c.size[k];
-                float4 rr = G.c.rot[k];
+                const float4 rr = G.c.rot[k];
                 S.c_rot[off] = make_float2(rr.x, rr.y);
                 S.c_lo[off] = make_float4(lo.x - kMargin, lo.y - kMargin, lo.z - kMargin, 0.0f);
                 S.c_hi[off] = make_float4(hi.x + kMargin, hi.y + kMargin, hi.z + kMargin, 0.0f);
@@ -361,19 +523,19 @@ __global__ void __launch_bounds__(kPeThreads, 2) pe_trace_kernel(PEParams P, Dev
     for (int k0 = 0; k0 < G.n_holes; k0 += kPeThreads) {
         const int k = k0 + tid;
         bool pass = false;
-        float4 ha, hb;
+        float4 ha = make_float4(0.f, 0.f, 0.f, 0.f), hb = ha;
         if (k < G.n_holes) {
             ha = G.h.a[k];
             hb = G.h.b[k];
-            Box3 K = hole_box(ha, hb);
+            const Box3 K = hole_box(ha, hb);
             for (int j = 0; j < n_d && !pass; ++j) pass = window_hit(A, S.d_box[j], K);
         }
-        unsigned bal = __ballot_sync(0xffffffffu, pass);
+        const unsigned bal = __ballot_sync(0xffffffffu, pass);
         if (lane == 0) S.warp_cnt[warp] = __popc(bal);
         __syncthreads();
         int off = base, total = 0;
         for (int w = 0; w < kPeWarps; ++w) {
-            int cnt = S.warp_cnt[w];
+            const int cnt = S.warp_cnt[w];
             if (w < warp) off += cnt;
             total += cnt;
         }
@@ -395,31 +557,26 @@ __global__ void __launch_bounds__(kPeThreads, 2) pe_trace_kernel(PEParams P, Dev
         S.n_c = n_c;
         S.n_h = n_h;
     }
-    if (tid <= G.n_plates) {
-        // First staged hole whose id is at or beyond plate `tid`'s first hole.
-        int first = (tid < G.n_plates) ? G.plate[tid].hole_begin : G.n_holes;
-        int cnt = 0;
-        for (int i = 0; i < n_h; ++i) cnt += (S.h_id[i] < first) ? 1 : 0;
-        S.h_plate_begin[tid] = cnt;
-    }
     __syncthreads();
 
     // ---- 2. per-warp crystal, voxel walk --------------------------------------
     const int tv = P.bx * P.by * P.bz;
     const int d = d0 + warp;
+    WarpLists& L = S.wl[warp];
     if (d < P.row1) {
         Detecting D;
-        D.id = d;
         {
-            float4 pos = G.c.pos[d], sz = G.c.size[d], rt = G.c.rot[d], ph = G.c.phys[d];
+            const float4 pos = G.c.pos[d], sz = G.c.size[d], rt = G.c.rot[d], ph = G.c.phys[d];
             D.cx = pos.x; D.cy = pos.y; D.cz = pos.z; D.mu_t = pos.w; D.mu_pe = ph.x;
             D.w = sz.x; D.t = sz.y; D.h = sz.z; D.crit = sz.w;
             D.cm = rt.x; D.sm = rt.y; D.cp = rt.z; D.sp = rt.w;
-            D.self_box = Box3{-D.w / 2.0f, -D.t / 2.0f, -D.h / 2.0f, D.w / 2.0f, D.t / 2.0f, D.h / 2.0f};
             D.world = S.d_box[warp];
             D.area_x = D.t * D.h / (float)P.dZ / (float)P.dY;
             D.area_z = D.w * D.t / (float)P.dX / (float)P.dY;
             D.area_y = D.w * D.h / (float)P.dX / (float)P.dZ;
+            D.hx = 0.5f * D.w / (float)P.dX;
+            D.hy = 0.5f * D.t / (float)P.dY;
+            D.hz = 0.5f * D.h / (float)P.dZ;
         }
         const bool absorbing = D.mu_t > 0.01f;   // PESysMatGen.cu:504, :598
         unsigned long long cnt_rays = 0, cnt_cry = 0, cnt_hole = 0, cnt_cone = 0;
@@ -432,53 +589,88 @@ __global__ void __launch_bounds__(kPeThreads, 2) pe_trace_kernel(PEParams P, Dev
             if (ix >= ix1 || iy >= iy1 || iz >= iz1) continue;
             int rec_slot = -1;
             if (RECORD) {
-                long long vox = ((long long)iz * P.ny + iy) * P.nx + ix;
+                const long long vox = ((long long)iz * P.ny + iy) * P.nx + ix;
                 for (int i = 0; i < P.rec_n; ++i)
                     if (P.rec_rows[i] == d && P.rec_vox[i] == vox) rec_slot = i;
                 if (rec_slot < 0) continue;
             }
             float acc = 0.0f, comp = 0.0f;
             if (absorbing) {
+                // Voxel-level candidate lists: staged crystals/holes the bundle from
+                // this voxel's sub-points to the crystal can reach.
+                {
+                    const Bundle bv = make_bundle(point_box_of(ix, iy, iz, ix + 1, iy + 1, iz + 1), D.world);
+                    int cnt = 0;
+                    for (int k0 = 0; k0 < n_c; k0 += 32) {
+                        const int k = k0 + lane;
+                        const bool pass = k < n_c && S.c_id[k] != d && bundle_hit(bv, box_of(S.c_lo[k], S.c_hi[k]));
+                        cnt = warp_append(pass, k, L.list_c, cnt, kListC, lane, P.status);
+                    }
+                    cnt = min(cnt, kListC);
+                    int cnth = 0;
+                    for (int k0 = 0; k0 < n_h; k0 += 32) {
+                        const int k = k0 + lane;
+                        const bool pass = k < n_h && bundle_hit(bv, hole_box(S.h_a[k], S.h_b[k]));
+                        cnth = warp_append(pass, k, L.list_h, cnth, kListH, lane, P.status);
+                    }
+                    cnth = min(cnth, kListH);
+                    __syncwarp();
+                    // First list index of each plate's holes (hole ids ascend with the plate).
+                    for (int m = 0; m <= G.n_plates; ++m) {
+                        const int first = (m < G.n_plates) ? G.plate[m].hole_begin : G.n_holes;
+                        int below = 0;
+                        for (int i0 = 0; i0 < cnth; i0 += 32) {
+                            const int i = i0 + lane;
+                            below += __popc(__ballot_sync(0xffffffffu, i < cnth && S.h_id[L.list_h[i]] < first));
+                        }
+                        if (lane == 0) L.plate_begin[m] = below;
+                    }
+                    if (lane == 0) {
+                        L.n_c = cnt;
+                        L.n_h = cnth;
+                    }
+                    __syncwarp();
+                }
+                const int lc = L.n_c, lh = L.n_h;
                 for (int s0 = 0; s0 < P.n_sv; s0 += P.group) {
                     const int gn = min(P.group, P.n_sv - s0);
-                    // Candidate masks for sub-points s0 .. s0+gn-1.
+                    // Candidate masks for sub-points s0 .. s0+gn-1 (cone test on the lists).
                     for (int j = 0; j < gn; ++j) {
-                        int fx, fy, fz;
-                        subpoint_index(P, ix, iy, iz, s0 + j, fx, fy, fz);
-                        const Vec3 p = subpoint(P, fx, fy, fz);
+                        const Vec3 p = subpoint_of(P, ix, iy, iz, s0 + j);
                         const ConeSelf cs = cone_self(D, p);
-                        const Box3 pb = point_box(p);
-                        for (int wd = 0; wd < kMaskC; ++wd) {
-                            if ((wd << 5) >= n_c) {
-                                if (lane == 0) S.mask[warp][j][wd] = 0u;
-                                continue;
-                            }
-                            const int k = (wd << 5) + lane;
+                        const Bundle bp = make_bundle(Box3{p.x, p.y, p.z, p.x, p.y, p.z}, D.world);
+                        for (int i0 = 0; i0 < lc; i0 += 32) {
+                            const int i = i0 + lane;
                             bool pass = false;
-                            if (k < n_c && S.c_id[k] != d && window_hit(pb, D.world, box_of(S.c_lo[k], S.c_hi[k]))) {
-                                const float4 kp = S.c_pos[k];
-                                pass = cone_crystal(cs, p, kp.x, kp.y, kp.z, S.c_size[k].w);
-                                if (P.counters) ++cnt_cone;
-                            }
-                            unsigned bal = __ballot_sync(0xffffffffu, pass);
-                            if (lane == 0) S.mask[warp][j][wd] = bal;
-                        }
-                        for (int wd = 0; wd < kMaskH; ++wd) {
-                            if ((wd << 5) >= n_h) {
-                                if (lane == 0) S.mask[warp][j][kMaskC + wd] = 0u;
-                                continue;
-                            }
-                            const int k = (wd << 5) + lane;
-                            bool pass = false;
-                            if (k < n_h) {
-                                const float4 ha = S.h_a[k], hb = S.h_b[k];
-                                if (window_hit(pb, D.world, hole_box(ha, hb))) {
-                                    pass = cone_hole(cs, p, ha.x, hb.w, ha.w, hb.z);
+                            if (i < lc) {
+                                const int k = L.list_c[i];
+                                if (bundle_hit(bp, box_of(S.c_lo[k], S.c_hi[k]))) {
+                                    const float4 kp = S.c_pos[k];
+                                    const float crit = S.c_size[k].w;
+                                    int f = cone_filter(cs, p, kp.x, kp.y, kp.z, 0.5f * crit);
+                                    if (f < 0) f = cone_crystal_exact(cs, p, kp.x, kp.y, kp.z, crit) ? 1 : 0;
+                                    pass = f > 0;
                                     if (P.counters) ++cnt_cone;
                                 }
                             }
-                            unsigned bal = __ballot_sync(0xffffffffu, pass);
-                            if (lane == 0) S.mask[warp][j][kMaskC + wd] = bal;
+                            const unsigned bal = __ballot_sync(0xffffffffu, pass);
+                            if (lane == 0) L.mask_c[j][i0 >> 5] = bal;
+                        }
+                        for (int i0 = 0; i0 < lh; i0 += 32) {
+                            const int i = i0 + lane;
+                            bool pass = false;
+                            if (i < lh) {
+                                const int k = L.list_h[i];
+                                const float4 ha = S.h_a[k], hb = S.h_b[k];
+                                if (bundle_hit(bp, hole_box(ha, hb))) {
+                                    int f = cone_filter(cs, p, ha.x, hb.w, ha.w, hb.z);
+                                    if (f < 0) f = cone_hole_exact(cs, p, ha.x, hb.w, ha.w, hb.z) ? 1 : 0;
+                                    pass = f > 0;
+                                    if (P.counters) ++cnt_cone;
+                                }
+                            }
+                            const unsigned bal = __ballot_sync(0xffffffffu, pass);
+                            if (lane == 0) L.mask_h[j][i0 >> 5] = bal;
                         }
                     }
                     __syncwarp();
@@ -486,11 +678,13 @@ __global__ void __launch_bounds__(kPeThreads, 2) pe_trace_kernel(PEParams P, Dev
                     for (int q0 = 0; q0 < nr; q0 += 32) {
                         const int q = q0 + lane;
                         if (q < nr) {
-                            const int j = q / P.n_sc;
+                            const int j = (gn == 1) ? 0 : fast_div(q, P.n_sc, P.inv_n_sc);
                             const int c = q - j * P.n_sc;
-                            int fx, fy, fz;
-                            subpoint_index(P, ix, iy, iz, s0 + j, fx, fy, fz);
-                            const Vec3 p = subpoint(P, fx, fy, fz);
+                            const int sz = fast_div(c, P.dX * P.dY, P.inv_dXdY);
+                            const int rem = c - sz * P.dX * P.dY;
+                            const int sx = fast_div(rem, P.dY, P.inv_dY);
+                            const int sy = rem - sx * P.dY;
+                            const Vec3 p = subpoint_of(P, ix, iy, iz, s0 + j);
                             Vec3 ps;
                             ps.x = (p.x - D.cx) * D.cm - (p.z - D.cz) * D.sm;
                             ps.y = p.y - D.cy;
@@ -499,11 +693,12 @@ __global__ void __launch_bounds__(kPeThreads, 2) pe_trace_kernel(PEParams P, Dev
                             if (RECORD)
                                 rec = P.rec_out + ((long long)rec_slot * P.n_sv * P.n_sc + (long long)(s0 + j) * P.n_sc + c) *
                                                       kRecWords;
-                            float v = trace_ray<RECORD>(P, G, S, S.mask[warp][j], D, p, ps, c, rec, P.status, pc_cry, pc_hole);
+                            const float v = trace_ray<RECORD>(P, G, S, L, L.mask_c[j], L.mask_h[j], D, p, ps, sx, sy, sz,
+                                                              rec, P.status, pc_cry, pc_hole);
                             if (P.counters) ++cnt_rays;
                             // Kahan summation of the lane's rays.
-                            float y = v - comp;
-                            float t = acc + y;
+                            const float y = v - comp;
+                            const float t = acc + y;
                             comp = (t - acc) - y;
                             acc = t;
                         }

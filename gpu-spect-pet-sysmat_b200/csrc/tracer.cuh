@@ -214,7 +214,7 @@ __device__ __forceinline__ float chord_hole(float xi, float yi, float zi, float 
 // lambda is monotone in y, a_y and b_y, so its range over K's depth band comes
 // from box corners.  Returns true whenever the ordering assumption fails.
 __device__ __forceinline__ bool window_hit(const Box3& A, const Box3& B, const Box3& K) {
-    if (K.y1 > B.y2) return false;               // every segment ends before K
+    if (K.y1 > fmaxf(A.y2, B.y2) || K.y2 < fminf(A.y1, B.y1)) return false;   // K outside every segment's depth range
     if (!(A.y2 < K.y1) || !(A.y2 < B.y1)) return true;
     float yhi = fminf(K.y2, B.y2);
     float lmin = (K.y1 - A.y2) / (B.y2 - A.y2);
