@@ -260,8 +260,8 @@ def run_ours(args, world, rank, local):
     nx, ny, nz = p.grid
     n_slabs = nz // SLAB_Z
     slab_vox = nx * ny * SLAB_Z
-    rows = p.n_crystals if args.rows <= 0 else min(args.rows, p.n_crystals)
-    row_range = (0, rows)
+    rows = p.n_crystals if args.rows <= 0 else min(args.rows, p.n_crystals - args.row0)
+    row_range = (0, rows) if args.rows <= 0 else (args.row0, args.row0 + rows)
     out = torch.empty((rows, slab_vox), dtype=torch.float32, device=dev)
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
     stream = torch.cuda.Stream(device=dev)
@@ -408,6 +408,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--ref-entries", type=int, default=4096)
     ap.add_argument("--rows", type=int, default=0, help="limit the crystal rows per step (profiling runs)")
+    ap.add_argument("--row0", type=int, default=0, help="first crystal row when --rows limits them")
     ap.add_argument("--no-ref-cuda", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
