@@ -73,6 +73,9 @@ PROTOTYPES = {
     "sm_pe_options_reference": (None, [ctypes.POINTER(PeOptions)]),
     "sm_pe_compute": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(PeOptions), ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                      ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int64, ctypes.c_int, _vp]),
+    "sm_pe_compute_static": (ctypes.c_int, [_f32p, ctypes.c_size_t, _f32p, ctypes.c_size_t, _f32p, ctypes.c_size_t,
+                                            ctypes.POINTER(PeOptions), ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                            ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int64, _vp]),
     "sm_pe_record_hits": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(PeOptions), ctypes.c_int, _i64p, _i64p,
                                          ctypes.c_int64, _i32p, ctypes.POINTER(ctypes.c_int)]),
     "sm_pe_set_counters": (ctypes.c_int, [_vp, ctypes.c_int]),
@@ -233,6 +236,22 @@ class Geometry:
                                        out.ctypes.data_as(_i32p), ctypes.byref(words)))
         w = words.value
         return out[:r.size * rays * w].reshape(r.size, rays, w)
+
+
+def pe_compute_static(p, dst_ptr: int, ld: int, rotation: int = 0, rows: Optional[Tuple[int, int]] = None,
+                      z: Optional[Tuple[int, int]] = None, opts: Optional[PeOptions] = None, stream: int = 0):
+    """Photoelectric sysmat through ``sm_pe_compute_static``, the entry point
+    that allocates no device memory (for callers that cannot call
+    cudaMalloc).  ``dst_ptr`` is a device pointer to (rows) x ``ld`` float32 on
+    the current device; the call returns when the block is written."""
+    col, det, img = _as_f32(p.collimator), _as_f32(p.detector), _as_f32(p.image)
+    nx, ny, nz_full = p.grid
+    r0, r1 = rows if rows is not None else (0, p.n_crystals)
+    z0, nz = z if z is not None else (0, nz_full)
+    opts = opts if opts is not None else PeOptions.make(p.sv, p.sc)
+    _check(lib().sm_pe_compute_static(_fptr(col), col.size, _fptr(det), det.size, _fptr(img), img.size,
+                                      ctypes.byref(opts), int(rotation), int(r0), int(r1), int(z0), int(nz),
+                                      _vp(int(dst_ptr)), int(ld), _vp(stream)))
 
 
 def primitive_batch(kind: str, args: np.ndarray) -> np.ndarray:

@@ -111,6 +111,30 @@ int sm_pe_compute(sm_context* ctx, const sm_geometry* geo, const sm_pe_options* 
                   int row0, int row1, int z0, int nz, float* dst, int64_t ld, int dst_on_device,
                   void* stream);
 
+/* No counterpart in the reference.  sm_pe_compute for callers that cannot
+ * allocate device memory: a host application that routes every device byte
+ * through its own pool or arena and forbids other allocators, a plugin loaded
+ * into such a process, or code that must not take the device-wide
+ * synchronisation cudaMalloc / cudaFree can cause.  It calls no cudaMalloc,
+ * cudaFree or other allocating routine: its working memory (derived geometry
+ * and status word) is a fixed 4 MiB __device__ array inside the library,
+ * held on every GPU that loads the library until the process exits.
+ *   - Tables are host arrays (lengths in floats) as for sm_geometry_create;
+ *     dst is device memory of the current device, dst[(r - row0) * ld + c]
+ *     as for sm_pe_compute; the call runs on the calling thread's current
+ *     device and on `stream` (NULL = legacy default stream).
+ *   - Geometries whose derived tables exceed the array (about 40000 crystals
+ *     with 2000 holes) are rejected with SM_ERR_CAPACITY.
+ *   - The first call on a device looks up the array's device address once
+ *     (set-up); make that first call before any stream capture.
+ *   - Every call shares the one array, which keeps the previous call's
+ *     contents; calls overlapping on the GPU would race, so the library runs
+ *     one call at a time per process and returns only after its kernel has
+ *     finished (it reads back the status word). */
+int sm_pe_compute_static(const float* collimator, size_t n_collimator, const float* detector, size_t n_detector,
+                         const float* image, size_t n_image, const sm_pe_options* opt, int rotation, int row0,
+                         int row1, int z0, int nz, float* dst, int64_t ld, void* stream);
+
 /* Diagnostic: for each listed entry (rows[i], voxels[i] as full-volume voxel
  * index) record every ray's hits exactly as the production kernel decides
  * them.  Per ray, `record_words` int32: [plate-miss mask, n_holes, holes
