@@ -1,0 +1,439 @@
+// Primary-Compton scatter kernels for sm_100a (see scatter.h for the split).
+//
+// Physics per (detector d, voxel I, scatter point S), as the reference's
+// crystalScatterSysMatCuda / collimatorScatterSysMatCuda
+// (ScatterGen_RayTracing_CircularHole/scatter.cu:1077-1437, :1544-1936):
+//   W(S, I) * RangePhi / 2pi * KNfraction(theta_min, theta_max) * P_window(E')
+//     * exp(-sum_k mu_k(E') L_k - mu_d(E') L_self) * (1 - exp(-mu_d(E') L_abs)) mu_pe,d(E') / mu_d(E')
+// with E' = E0 / (1 + alpha (1 - cos theta)), theta the angle at S between
+// I -> S and S -> D, mu_pe(E') = mu_pe (E0/E')^3, mu_c(E') = mu_c E0/E'.
+// W is PE[s, I] mu_c,d / mu_pe,d (crystal scatter) or the virtual solid angle
+// of the hole times mu_c / mu_t of plate 0 (collimator scatter).
+//
+// Differences in arithmetic (not in the quantities): the cosine and sine of
+// the scatter angle come from a dot and a cross product instead of
+// cos(acos(.)), the polar range from atan2 of the extreme unit-box corners
+// instead of eight acos, and the reference's 0.01 rad rectangle sum of the
+// Klein-Nishina integrand (up to 315 terms) from a closed form: the
+// Euler-Maclaurin formula with the exact integral (a Taylor table of
+// g = KN sin theta, built in double on the host) and its first two
+// correction terms, whose remainder is below 1e-10.
+#include <algorithm>
+
+#include <cuda_runtime.h>
+
+#include "scatter.h"
+#include "scatter_term.cuh"
+#include "tracer.cuh"
+
+namespace smb {
+namespace {
+
+
+// ---- bitmaps (scatter.cu:1440-1540, :1939-2009) ------------------------------
+// Single-precision expressions in the reference's order; this translation
+// unit is compiled without fused multiply-add, so every bit matches.
+__device__ __forceinline__ float dist3(float x1, float y1, float z1, float x2, float y2, float z2) {
+    return sqrtf((x1 - x2) * (x1 - x2) + (y1 - y2) * (y1 - y2) + (z1 - z2) * (z1 - z2));
+}
+
+__device__ bool crystal_bit(const float4* cr, int i, int j, int k) {
+    const float4 a = cr[i], b = cr[j], c = cr[k];
+    const float Lij = dist3(a.x, a.y, a.z, b.x, b.y, b.z);
+    const float crit_ij = a.w / Lij, crit_ji = b.w / Lij;
+    const float ex_ij = (a.x - b.x) / Lij, ey_ij = (a.y - b.y) / Lij, ez_ij = (a.z - b.z) / Lij;
+    const float ex_ji = (b.x - a.x) / Lij, ey_ji = (b.y - a.y) / Lij, ez_ji = (b.z - a.z) / Lij;
+    const float Lik = dist3(c.x, c.y, c.z, a.x, a.y, a.z);
+    const float crit_ki = c.w / Lik;
+    const float Ljk = dist3(c.x, c.y, c.z, b.x, b.y, b.z);
+    const float crit_kj = c.w / Ljk;
+    const float ex_ki = (c.x - a.x) / Lik, ey_ki = (c.y - a.y) / Lik, ez_ki = (c.z - a.z) / Lik;
+    const float ex_kj = (c.x - b.x) / Ljk, ey_kj = (c.y - b.y) / Ljk, ez_kj = (c.z - b.z) / Ljk;
+    if (dist3(ex_ki, ey_ki, ez_ki, ex_ji, ey_ji, ez_ji) <= crit_ki + crit_ji) return true;
+    return dist3(ex_kj, ey_kj, ez_kj, ex_ij, ey_ij, ez_ij) <= crit_kj + crit_ij;
+}
+
+__device__ bool collimator_bit(const float4* cr, const float4* hr, int i, int j, int k) {
+    const float4 h = hr[i], b = cr[j], c = cr[k];
+    const float Lij = dist3(h.x, h.y, h.z, b.x, b.y, b.z);
+    const float crit_ji = b.w / Lij;
+    const float ex_ji = (b.x - h.x) / Lij, ey_ji = (b.y - h.y) / Lij, ez_ji = (b.z - h.z) / Lij;
+    const float Lik = dist3(c.x, c.y, c.z, h.x, h.y, h.z);
+    const float crit_ki = c.w / Lik;
+    const float ex_ki = (c.x - h.x) / Lik, ey_ki = (c.y - h.y) / Lik, ez_ki = (c.z - h.z) / Lik;
+    return dist3(ex_ki, ey_ki, ez_ki, ex_ji, ey_ji, ez_ji) <= crit_ki + crit_ji;
+}
+
+// Pair index (i <= j) -> i: the largest i with i*N - i*(i-1)/2 <= pair.
+__device__ __forceinline__ int pair_row(long long pair, int N) {
+    const double b = 2.0 * N + 1.0;
+    int i = (int)((b - sqrt(b * b - 8.0 * (double)pair)) * 0.5);
+    if (i < 0) i = 0;
+    auto start = [N](long long r) { return r * N - r * (r - 1) / 2; };
+    while (i > 0 && start(i) > pair) --i;
+    while (i + 1 < N && start(i + 1) <= pair) ++i;
+    return i;
+}
+
+// One thread per 32-bit word: bits bit0 .. bit0 + 31 of the pair-major bitmap
+// bit = (i N - i (i + 1) / 2 + j) N + k, i <= j; set for i < j, k != i, j.
+__global__ void bitmap_crystal_kernel(uint32_t* words, long long n_words, ScatterTables T) {
+    const int N = T.n_crystals;
+    const long long total = ((long long)N * (N + 1) / 2) * N;
+    for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < n_words;
+         w += (long long)gridDim.x * blockDim.x) {
+        const long long bit0 = w * 32;
+        long long pair = bit0 / N;
+        int k = (int)(bit0 - pair * N);
+        int i = pair_row(pair, N);
+        int j = (int)(pair - ((long long)i * N - (long long)i * (i - 1) / 2)) + i;
+        uint32_t word = 0u;
+        for (int b = 0; b < 32 && bit0 + b < total; ++b) {
+            if (i < j && k != i && k != j && crystal_bit(T.crystal_raw, i, j, k)) word |= 1u << b;
+            if (++k == N) {
+                k = 0;
+                if (++j == N) {
+                    ++i;
+                    j = i;
+                }
+            }
+        }
+        words[w] = word;
+    }
+}
+
+// bit = i N^2 + j N + k for layer-0 hole i, crystals j, k.
+__global__ void bitmap_collimator_kernel(uint32_t* words, long long n_words, ScatterTables T) {
+    const int N = T.n_crystals;
+    const long long total = (long long)T.n_holes0 * N * N;
+    for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < n_words;
+         w += (long long)gridDim.x * blockDim.x) {
+        const long long bit0 = w * 32;
+        int i = (int)(bit0 / ((long long)N * N));
+        long long rem = bit0 - (long long)i * N * N;
+        int j = (int)(rem / N);
+        int k = (int)(rem - (long long)j * N);
+        uint32_t word = 0u;
+        for (int b = 0; b < 32 && bit0 + b < total; ++b) {
+            if (collimator_bit(T.crystal_raw, T.hole_raw, i, j, k)) word |= 1u << b;
+            if (++k == N) {
+                k = 0;
+                if (++j == N) {
+                    j = 0;
+                    ++i;
+                }
+            }
+        }
+        words[w] = word;
+    }
+}
+
+// ---- per (scatter point, detector) ---------------------------------------------
+// sum_k L_k mu_pe_k, sum_k L_k mu_c_k over the crystals k the bitmap flags for
+// the pair (scatter.cu:1309-1367, :1832-1889), the path inside the detecting
+// crystal before its unit (:1371-1382), and the absorption chord (:1385-1392).
+// The detector unit is the whole crystal (the reference's divide = 1), whose
+// centre is the crystal centre.
+template <int KIND>
+__global__ void scatter_pair_kernel(DevGeometry G, ScatterTables T, const uint32_t* __restrict__ bitmap, int d0,
+                                    int d1, float4* __restrict__ pair, int n_sources) {
+    const int N = T.n_crystals;
+    const int d = d0 + blockIdx.x * blockDim.x + threadIdx.x;
+    if (d >= d1) return;
+    const long long ld = d1 - d0;
+    const float4 Dp = G.c.pos[d], Dsz = G.c.size[d], Dr = G.c.rot[d];
+    for (int q = blockIdx.y; q < n_sources; q += gridDim.y) {
+        float4 S;
+        int s;
+        if (KIND == kScatterCrystal) {
+            S = T.crystal_src[q];
+            s = q / T.n_points;
+        } else {
+            S = T.hole_src[q];
+            s = q;
+        }
+        float4 out = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (!(KIND == kScatterCrystal && s == d)) {
+            float a_pe = 0.0f, a_c = 0.0f;
+            long long base;
+            if (KIND == kScatterCrystal) {
+                const int lo = s < d ? s : d, hi = s < d ? d : s;
+                base = ((long long)lo * N - (long long)lo * (lo + 1) / 2 + hi) * N;
+            } else {
+                base = ((long long)s * N + d) * N;
+            }
+            const long long w_end = (base + N - 1) >> 5;
+            for (long long wi = base >> 5; wi <= w_end; ++wi) {
+                uint32_t bits = __ldg(bitmap + wi);
+                const long long first = wi << 5;
+                if (first < base) bits &= ~0u << (int)(base - first);
+                if (first + 31 > base + N - 1) {
+                    const int keep = (int)(base + N - first);
+                    bits &= keep >= 32 ? ~0u : ((1u << keep) - 1u);
+                }
+                while (bits) {
+                    const int b = __ffs(bits) - 1;
+                    bits &= bits - 1u;
+                    const int k = (int)(first + b - base);
+                    if (k == d || (KIND == kScatterCrystal && k == s)) continue;
+                    const float4 kp = G.c.pos[k], ks = G.c.size[k], kr = G.c.rot[k], kph = G.c.phys[k];
+                    const float xa = (S.x - kp.x) * kr.x - (S.z - kp.z) * kr.y;
+                    const float ya = S.y - kp.y;
+                    const float za = (S.x - kp.x) * kr.y + (S.z - kp.z) * kr.x;
+                    const float xb = (Dp.x - kp.x) * kr.x - (Dp.z - kp.z) * kr.y;
+                    const float yb = Dp.y - kp.y;
+                    const float zb = (Dp.x - kp.x) * kr.y + (Dp.z - kp.z) * kr.x;
+                    const Box3 kb{-0.5f * ks.x, -0.5f * ks.y, -0.5f * ks.z, 0.5f * ks.x, 0.5f * ks.y, 0.5f * ks.z};
+                    const float len = chord_through(xa, ya, za, xb, yb, zb, kb);
+                    a_pe += len * kph.x;
+                    a_c += len * kph.y;
+                }
+            }
+            // scatter point in the detecting crystal's frame
+            const float xs = (S.x - Dp.x) * Dr.x - (S.z - Dp.z) * Dr.y;
+            const float ys = S.y - Dp.y;
+            const float zs = (S.x - Dp.x) * Dr.y + (S.z - Dp.z) * Dr.x;
+            const Box3 cb{-Dsz.x / 2.0f, -Dsz.y / 2.0f, -Dsz.z / 2.0f, Dsz.x / 2.0f, Dsz.y / 2.0f, Dsz.z / 2.0f};
+            const Box3 ub{-0.5f * Dsz.x, -0.5f * Dsz.y, -0.5f * Dsz.z, 0.5f * Dsz.x, 0.5f * Dsz.y, 0.5f * Dsz.z};
+            const float l1 = chord_to_end(xs, ys, zs, 0.0f, 0.0f, 0.0f, cb);
+            const float l2 = chord_to_end(xs, ys, zs, 0.0f, 0.0f, 0.0f, ub);
+            const float L = dist3(S.x, S.y, S.z, Dp.x, Dp.y, Dp.z);
+            const float xt = 0.0f + 1000.0f * (0.0f - xs) / L;
+            const float yt = 0.0f + 1000.0f * (0.0f - ys) / L;
+            const float zt = 0.0f + 1000.0f * (0.0f - zs) / L;
+            const float labs = chord_through(xs, ys, zs, xt, yt, zt, ub);
+            out = make_float4(a_pe, a_c, l1 - l2, labs);
+        }
+        pair[(long long)q * ld + (d - d0)] = out;
+    }
+}
+
+// ---- sources with PE != 0 per voxel brick -----------------------------------------
+__global__ void brick_sources_kernel(ScatterParams P, int N, uint32_t* __restrict__ out) {
+    const int b = blockIdx.x;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int s = blockIdx.y * kScWarps + warp;
+    if (s >= N) return;
+    const int bx = b % P.bricks_x, by = (b / P.bricks_x) % P.bricks_y, bz = b / (P.bricks_x * P.bricks_y);
+    const int x = bx * kScBrickX + (lane & 7);
+    bool any = false;
+    for (int it = 0; it < kScBrickY / 4; ++it) {
+        const int y = by * kScBrickY + it * 4 + (lane >> 3);
+        if (x < P.nx && y < P.ny) {
+            const long long v = (long long)x + (long long)P.nx * (y + (long long)P.ny * bz);
+            any |= __ldg(P.pe + (long long)s * P.ld_pe + v) != 0.0f;
+        }
+    }
+    if (__any_sync(0xffffffffu, any) && lane == 0) atomicOr(out + (long long)b * P.src_words + (s >> 5), 1u << (s & 31));
+}
+
+struct __align__(16) ScSmem {
+    KnNode kn[kKnNodes + 1];
+    double acc[kScBrickX][kScBrickY][kScTileD];
+    float4 vox[kScBrickX][kScBrickY];          // voxel centres (world); w < 0 marks outside the grid
+    float pe[kScBrickY][kScBrickX];
+    float scale[kScTileD];                     // per detector: mu_c / mu_pe / points, or plate mu_c / mu_t
+};
+
+template <int KIND>
+__global__ void __launch_bounds__(kScThreads, 2) scatter_main_kernel(ScatterParams P, DevGeometry G, ScatterTables T) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    ScSmem& S = *reinterpret_cast<ScSmem*>(smem_raw);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int b = blockIdx.x % P.n_bricks;
+    const int dt = blockIdx.x / P.n_bricks;
+    const int bx = b % P.bricks_x, by = (b / P.bricks_x) % P.bricks_y, bz = b / (P.bricks_x * P.bricks_y);
+    const int x0 = bx * kScBrickX, y0 = by * kScBrickY;
+
+    for (int i = tid; i < kKnNodes + 1; i += kScThreads) S.kn[i] = T.kn[i];
+    for (int i = tid; i < kScBrickX * kScBrickY * kScTileD; i += kScThreads) (&S.acc[0][0][0])[i] = 0.0;
+    {
+        const int xx = tid & 7, yy = tid >> 3;
+        const int x = x0 + xx, y = y0 + yy;
+        float4 v = make_float4(0.0f, 0.0f, 0.0f, -1.0f);
+        if (x < P.nx && y < P.ny) {
+            // voxel centre, FOV shift, image rotation (scatter.cu:1172-1184)
+            float xi = ((float)x - (float)P.nx / 2.0f + 0.5f) * P.vx;
+            float yi = ((float)y - (float)P.ny / 2.0f + 0.5f) * P.vy;
+            float zi = ((float)bz - (float)P.nz / 2.0f + 0.5f) * P.vz;
+            xi = xi + P.shx;
+            yi = yi + P.shy;
+            zi = zi + P.shz;
+            v = make_float4(xi * P.cos_a - yi * P.sin_a, xi * P.sin_a + yi * P.cos_a, zi, 1.0f);
+        }
+        S.vox[xx][yy] = v;
+    }
+
+    const int d = P.row0 + dt * kScTileD + lane;
+    Det D;
+    D.on = d < P.row1;
+    float scale = 0.0f;
+    if (D.on) {
+        const float4 pos = G.c.pos[d], sz = G.c.size[d], rt = G.c.rot[d], ph = G.c.phys[d];
+        D.x = pos.x; D.y = pos.y; D.z = pos.z; D.cm = rt.x; D.sm = rt.y;
+        D.hw = 0.5f * sz.x; D.ht = 0.5f * sz.y; D.hh = 0.5f * sz.z;
+        D.r_unit = sqrtf(sz.x * sz.x / 1.0f / 1.0f + sz.z * sz.z / 1.0f / 1.0f + sz.y * sz.y / 1.0f / 1.0f) / 2.0f;
+        D.mu_pe = ph.x; D.mu_c = ph.y; D.res = ph.z;
+        if (P.same_window > 0) { D.lo = P.win_lo; D.hi = P.win_hi; }
+        else {
+            D.lo = (1.0f - D.res / 2.0f) * P.e0;
+            D.hi = (1.0f + D.res / 2.0f) * P.e0;
+        }
+        D.on = P.use_compton == 1 && pos.w > 0.01f;   // (scatter.cu:1203-1205)
+        scale = KIND == kScatterCrystal ? D.mu_c / D.mu_pe / (float)T.n_points : P.plate_c_over_t;
+    }
+    if (warp == 0) S.scale[lane] = scale;
+    __syncthreads();
+
+    const int x = x0 + warp;
+    const float inv_norm = T.kn_inv_norm;
+    if (KIND == kScatterCrystal) {
+        const uint32_t* srcw = P.brick_sources + (long long)b * P.src_words;
+        for (int wd = 0; wd < P.src_words; ++wd) {
+            uint32_t bits = srcw[wd];
+            while (bits) {
+                const int s = (wd << 5) + __ffs(bits) - 1;
+                bits &= bits - 1u;
+                __syncthreads();
+                {
+                    const int xx = tid & 7, yy = tid >> 3;
+                    float v = 0.0f;
+                    if (x0 + xx < P.nx && y0 + yy < P.ny)
+                        v = __ldg(P.pe + (long long)s * P.ld_pe + (x0 + xx) + (long long)P.nx * ((y0 + yy) + (long long)P.ny * bz));
+                    S.pe[yy][xx] = v;
+                }
+                __syncthreads();
+                const float my_pe = S.pe[lane][warp];
+                const unsigned live = __ballot_sync(0xffffffffu, my_pe != 0.0f);
+                if (!live) continue;
+                for (int p = 0; p < T.n_points; ++p) {
+                    const int q = s * T.n_points + p;
+                    const float4 src = T.crystal_src[q];
+                    Src C;
+                    const float4 pr = D.on ? P.pair[(long long)q * P.pair_ld + (d - P.pair_d0)] : make_float4(0.f, 0.f, 0.f, 0.f);
+                    make_src(D, src, pr, C);
+                    const bool on = D.on && s != d;
+                    unsigned m = live;
+                    while (m) {
+                        const int j = __ffs(m) - 1;
+                        m &= m - 1u;
+                        const float w = __shfl_sync(0xffffffffu, my_pe, j);
+                        if (!on) continue;
+                        const float4 I = S.vox[warp][j];
+                        const float isx = (I.x - D.x) * D.cm - (I.z - D.z) * D.sm;
+                        const float isy = I.y - D.y;
+                        const float isz = (I.x - D.x) * D.sm + (I.z - D.z) * D.cm;
+                        const float t = scatter_term(P, D, C, S.kn, inv_norm, I.x, I.y, I.z, isx, isy, isz);
+                        S.acc[warp][j][lane] += (double)(w * t);
+                    }
+                }
+            }
+        }
+    } else {
+        for (int h = 0; h < T.n_holes0; ++h) {
+            const float4 src = T.hole_src[h];
+            Src C;
+            const float4 pr = D.on ? P.pair[(long long)h * P.pair_ld + (d - P.pair_d0)] : make_float4(0.f, 0.f, 0.f, 0.f);
+            make_src(D, src, pr, C);
+            if (!D.on || x >= P.nx) continue;
+            for (int j = 0; j < kScBrickY; ++j) {
+                const float4 I = S.vox[warp][j];
+                if (I.w < 0.0f) break;
+                // virtual solid angle of the hole seen from the voxel (scatter.cu:1707-1713)
+                const float vr = 0.1f;
+                const float dx = I.x - src.x, dy = I.y - src.y, dz = I.z - src.z;
+                const float L2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                const float Lih = sqrtf(L2);
+                const float w = (vr * vr * 3.14159265358979323846f + src.w * vr) /
+                                (4.0f * 3.14159265358979323846f * L2) * fabsf(src.y - I.y) / Lih;
+                const float isx = (I.x - D.x) * D.cm - (I.z - D.z) * D.sm;
+                const float isy = I.y - D.y;
+                const float isz = (I.x - D.x) * D.sm + (I.z - D.z) * D.cm;
+                const float t = scatter_term(P, D, C, S.kn, inv_norm, I.x, I.y, I.z, isx, isy, isz);
+                S.acc[warp][j][lane] += (double)(w * t);
+            }
+        }
+    }
+    __syncthreads();
+
+    // write the tile: (detector, y, 8 x) with x fastest
+    const int n_rows = min(kScTileD, P.row1 - (P.row0 + dt * kScTileD));
+    for (int i = tid; i < n_rows * kScBrickY * kScBrickX; i += kScThreads) {
+        const int xx = i & 7, yy = (i >> 3) & 31, dl = i >> 8;
+        const int xv = x0 + xx, yv = y0 + yy;
+        if (xv >= P.nx || yv >= P.ny) continue;
+        const int dd = P.row0 + dt * kScTileD + dl;
+        const float sc = S.scale[dl];
+        const long long col = (long long)xv + (long long)P.nx * (yv + (long long)P.ny * bz);
+        float* out = P.dst + (long long)(dd - P.row0) * P.ld + col;
+        const float v = (float)S.acc[xx][yy][dl] * sc;
+        *out = P.accumulate ? *out + v : v;
+    }
+}
+
+}  // namespace
+
+int64_t crystal_bitmap_words(int n) {
+    const int64_t bits = ((int64_t)n * (n + 1) / 2) * n;
+    return (bits + 31) / 32;
+}
+
+int64_t collimator_bitmap_words(int n, int h0) {
+    const int64_t bits = (int64_t)h0 * n * n;
+    return (bits + 31) / 32;
+}
+
+cudaError_t launch_bitmap_crystal(uint32_t* words, int64_t n_words, const ScatterTables& T, cudaStream_t s) {
+    if (n_words <= 0) return cudaSuccess;
+    const long long blocks = std::min<long long>((n_words + 255) / 256, 148LL * 64);
+    bitmap_crystal_kernel<<<(unsigned)blocks, 256, 0, s>>>(words, n_words, T);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_bitmap_collimator(uint32_t* words, int64_t n_words, const ScatterTables& T, cudaStream_t s) {
+    if (n_words <= 0) return cudaSuccess;
+    const long long blocks = std::min<long long>((n_words + 255) / 256, 148LL * 64);
+    bitmap_collimator_kernel<<<(unsigned)blocks, 256, 0, s>>>(words, n_words, T);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_scatter_pairs(int kind, const DevGeometry& G, const ScatterTables& T, const uint32_t* bitmap,
+                                 int d0, int d1, float4* pair, cudaStream_t s) {
+    const int n_src = kind == kScatterCrystal ? T.n_crystals * T.n_points : T.n_holes0;
+    if (d1 <= d0 || n_src <= 0) return cudaSuccess;
+    dim3 grid((d1 - d0 + 127) / 128, std::min(n_src, 65535));
+    if (kind == kScatterCrystal)
+        scatter_pair_kernel<kScatterCrystal><<<grid, 128, 0, s>>>(G, T, bitmap, d0, d1, pair, n_src);
+    else
+        scatter_pair_kernel<kScatterCollimator><<<grid, 128, 0, s>>>(G, T, bitmap, d0, d1, pair, n_src);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_brick_sources(const ScatterParams& P, const ScatterTables& T, uint32_t* brick_sources,
+                                 cudaStream_t s) {
+    dim3 grid(P.n_bricks, (T.n_crystals + kScWarps - 1) / kScWarps);
+    brick_sources_kernel<<<grid, kScThreads, 0, s>>>(P, T.n_crystals, brick_sources);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_scatter_main(const ScatterParams& P, const DevGeometry& G, const ScatterTables& T,
+                                cudaStream_t s) {
+    const size_t smem = sizeof(ScSmem);
+    const long long d_tiles = (P.row1 - P.row0 + kScTileD - 1) / kScTileD;
+    const long long blocks = d_tiles * P.n_bricks;
+    if (blocks <= 0) return cudaSuccess;
+    if (blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+    cudaError_t e;
+    if (P.kind == kScatterCrystal) {
+        e = cudaFuncSetAttribute(scatter_main_kernel<kScatterCrystal>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        scatter_main_kernel<kScatterCrystal><<<(unsigned)blocks, kScThreads, smem, s>>>(P, G, T);
+    } else {
+        e = cudaFuncSetAttribute(scatter_main_kernel<kScatterCollimator>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        scatter_main_kernel<kScatterCollimator><<<(unsigned)blocks, kScThreads, smem, s>>>(P, G, T);
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace smb

@@ -9,7 +9,15 @@
 // a better-conditioned form, the better form is used and says so.
 #pragma once
 
+#include <cmath>
+
 #include <cuda_runtime.h>
+
+// Host and device: the kernels use these, and host-side checks of the
+// kernels' arithmetic call the same code.
+#ifndef SM_HD
+#define SM_HD __host__ __device__ __forceinline__
+#endif
 
 namespace smb {
 
@@ -23,7 +31,7 @@ struct Box3 {
 
 // Entry/exit parameters of one slab for a segment parameterised by length
 // t_total (PESysMatGen.cu:57-64 and every slab of :19-151).
-__device__ __forceinline__ void slab_pair(float a_in, float a_out, float lo, float hi, float t_total, float& t_lo,
+SM_HD void slab_pair(float a_in, float a_out, float lo, float hi, float t_total, float& t_lo,
                                           float& t_hi) {
     float inv = t_total / (a_out - a_in);
     if (inv < 0.0f) {
@@ -36,7 +44,7 @@ __device__ __forceinline__ void slab_pair(float a_in, float a_out, float lo, flo
 }
 
 // Intersection of two slabs; false when they are disjoint.
-__device__ __forceinline__ bool slab_2d(float a_in, float a_out, float a_lo, float a_hi, float b_in, float b_out,
+SM_HD bool slab_2d(float a_in, float a_out, float a_lo, float a_hi, float b_in, float b_out,
                                         float b_lo, float b_hi, float t_total, float& tmin, float& tmax) {
     float ta0, ta1, tb0, tb1;
     slab_pair(a_in, a_out, a_lo, a_hi, t_total, ta0, ta1);
@@ -51,7 +59,7 @@ __device__ __forceinline__ bool slab_2d(float a_in, float a_out, float a_lo, flo
 // Returns 0 for "no overlap", 1 for an overlap [tmin, tmax] of a segment of
 // length t_total; the axis-degenerate answers (a full box side) come back as
 // code 2 with the length in tmax.
-__device__ __forceinline__ int slab_segment(float xi, float yi, float zi, float xo, float yo, float zo, const Box3& b,
+SM_HD int slab_segment(float xi, float yi, float zi, float xo, float yo, float zo, const Box3& b,
                                             bool inside_variant, float& tmin, float& tmax, float& t_total) {
     const float eps = 0.001f;
     bool cx = fabsf(xo - xi) < eps, cy = fabsf(yo - yi) < eps, cz = fabsf(zo - zi) < eps;
@@ -116,7 +124,7 @@ __device__ __forceinline__ int slab_segment(float xi, float yi, float zi, float 
 
 // Chord of segment a -> b through box, counted only if the segment enters and
 // leaves strictly inside (PESysMatGen.cu:19-151).
-__device__ __forceinline__ float chord_through(float xi, float yi, float zi, float xo, float yo, float zo,
+SM_HD float chord_through(float xi, float yi, float zi, float xo, float yo, float zo,
                                                const Box3& b) {
     const float eps = 0.001f;
     float tmin = 0.0f, tmax = 0.0f, t_total = 0.0f;
@@ -131,7 +139,7 @@ __device__ __forceinline__ float chord_through(float xi, float yi, float zi, flo
 
 // Chord from the box entry to the end of the segment inside the box
 // (PESysMatGen.cu:153-307).
-__device__ __forceinline__ float chord_to_end(float xi, float yi, float zi, float xo, float yo, float zo,
+SM_HD float chord_to_end(float xi, float yi, float zi, float xo, float yo, float zo,
                                               const Box3& b) {
     const float eps = 0.001f;
     if (fabsf(yo - yi) < 0.001f) return 0.0f;
@@ -154,7 +162,7 @@ __device__ __forceinline__ float chord_to_end(float xi, float yi, float zi, floa
 // the value t2 - t1 comes from a double-precision discriminant when it is
 // small relative to its terms (near-tangent rays), where the single-precision
 // difference (kx^2+kz^2)R^2 - (kx z - kz x)^2 cancels.
-__device__ __forceinline__ float chord_hole(float xi, float yi, float zi, float xo, float yo, float zo, float xc,
+SM_HD float chord_hole(float xi, float yi, float zi, float xo, float yo, float zo, float xc,
                                             float y1, float y2, float zc, float R) {
     if (fabsf(y1 - y2) < 0.001f) return 0.0f;
     float t_total = sqrtf((xo - xi) * (xo - xi) + (yo - yi) * (yo - yi) + (zo - zi) * (zo - zi));

@@ -50,6 +50,21 @@ class PeOptions(ctypes.Structure):
         return o
 
 
+class ScatterOptions(ctypes.Structure):
+    _fields_ = [("sp", ctypes.c_int * 3), ("parts", ctypes.c_int), ("flags", ctypes.c_int)]
+
+    @staticmethod
+    def make(sp=(1, 1, 1), parts: int = 3) -> "ScatterOptions":
+        o = ScatterOptions()
+        for i in range(3):
+            o.sp[i] = int(sp[i])
+        o.parts = int(parts)
+        o.flags = 0
+        return o
+
+
+SCATTER_PARTS = {"crystal": 1, "collimator": 2, "both": 3}
+
 _lib = None
 _f32p = ctypes.POINTER(ctypes.c_float)
 _i64p = ctypes.POINTER(ctypes.c_int64)
@@ -81,6 +96,14 @@ PROTOTYPES = {
     "sm_pe_set_counters": (ctypes.c_int, [_vp, ctypes.c_int]),
     "sm_pe_last_counters": (ctypes.c_int, [_vp, _i64p]),
     "sm_primitive_batch": (ctypes.c_int, [ctypes.c_int, _f32p, ctypes.c_int64, _f32p]),
+    "sm_scatter_options_reference": (None, [ctypes.POINTER(ScatterOptions)]),
+    "sm_scatter_bitmap_words": (ctypes.c_int, [_vp, _i64p]),
+    "sm_scatter_bitmaps": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_int, _vp]),
+    "sm_scatter_compute": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(ScatterOptions), ctypes.c_int, _vp,
+                                          ctypes.c_int64, ctypes.c_int, _vp, _vp, ctypes.c_int, ctypes.c_int,
+                                          ctypes.c_int, _vp, ctypes.c_int64, ctypes.c_int, _vp]),
+    "sm_scatter_legacy": (ctypes.c_int, [ctypes.c_int, _f32p, _f32p, _f32p, _f32p, _f32p, ctypes.c_char_p,
+                                         ctypes.c_char_p, _f32p, ctypes.c_int]),
 }
 
 
@@ -222,6 +245,65 @@ class Geometry:
                                    int(z0), int(nz), _vp(int(out)), int(ld), 1, _vp(stream)))
         return None
 
+    # ---- primary-Compton scatter -------------------------------------------
+
+    def bitmap_words(self) -> Tuple[int, int]:
+        out = np.zeros(2, dtype=np.int64)
+        _check(lib().sm_scatter_bitmap_words(self.handle, out.ctypes.data_as(_i64p)))
+        return int(out[0]), int(out[1])
+
+    def scatter_bitmaps(self) -> Tuple[np.ndarray, np.ndarray]:
+        """The crystal and collimator bitmaps (uint32 words, the reference's file format)."""
+        wc, wh = self.bitmap_words()
+        c = np.zeros(max(wc, 1), dtype=np.uint32)
+        h = np.zeros(max(wh, 1), dtype=np.uint32)
+        _check(lib().sm_scatter_bitmaps(self.ctx.handle, self.handle, _vp(c.ctypes.data),
+                                        _vp(h.ctypes.data) if wh > 0 else None, 0, None))
+        return c[:wc], h[:wh]
+
+    def scatter(self, pe=None, rotation: int = 0, sp=(1, 1, 1), parts="both", rows: Optional[Tuple[int, int]] = None,
+                bitmaps: Optional[Tuple[np.ndarray, np.ndarray]] = None, out=None, ld: Optional[int] = None,
+                pe_ld: Optional[int] = None, stream: int = 0) -> Optional[np.ndarray]:
+        """Primary-Compton scatter sysmat block [rows][voxels].
+
+        ``pe``: the rotation's PE sysmat, a host float32 array [N][V] or an
+        integer device pointer (then ``pe_ld`` gives its row pitch).  ``out``:
+        None (a host array is returned), a host array, or an integer device
+        pointer (asynchronous on ``stream`` when ``pe`` is on the device).
+        ``bitmaps``: optional host word arrays (crystal, collimator) as read
+        from the reference's files; computed on the device when omitted.
+        """
+        opt = ScatterOptions.make(sp, SCATTER_PARTS[parts] if isinstance(parts, str) else parts)
+        r0, r1 = rows if rows is not None else (0, self.n_crystals)
+        V = self.nx * self.ny * self.nz
+        ld = V if ld is None else ld
+        pe_ptr, pe_dev, pe_ld_v = None, 0, V
+        if pe is not None:
+            if isinstance(pe, np.ndarray):
+                pe_arr = np.ascontiguousarray(pe, dtype=np.float32)
+                if pe_arr.size < self.n_crystals * V:
+                    raise SysmatError(-1, "pe must hold N x V floats")
+                pe_ptr, pe_ld_v = _vp(pe_arr.ctypes.data), pe_arr.size // self.n_crystals
+            else:
+                pe_ptr, pe_dev, pe_ld_v = _vp(int(pe)), 1, (V if pe_ld is None else int(pe_ld))
+        bm_c = bm_h = None
+        if bitmaps is not None:
+            bc = np.ascontiguousarray(bitmaps[0], dtype=np.uint32)
+            bh = np.ascontiguousarray(bitmaps[1], dtype=np.uint32)
+            bm_c, bm_h = _vp(bc.ctypes.data), (_vp(bh.ctypes.data) if bh.size else None)
+        if out is None or isinstance(out, np.ndarray):
+            host = np.zeros((r1 - r0, ld), dtype=np.float32) if out is None else out
+            if host.dtype != np.float32 or not host.flags.c_contiguous or host.size < (r1 - r0) * ld:
+                raise SysmatError(-1, "out must be C-contiguous float32 with rows*ld elements")
+            _check(lib().sm_scatter_compute(self.ctx.handle, self.handle, ctypes.byref(opt), int(rotation), pe_ptr,
+                                            int(pe_ld_v), pe_dev, bm_c, bm_h, 0, int(r0), int(r1),
+                                            _vp(host.ctypes.data), int(ld), 0, _vp(stream)))
+            return host
+        _check(lib().sm_scatter_compute(self.ctx.handle, self.handle, ctypes.byref(opt), int(rotation), pe_ptr,
+                                        int(pe_ld_v), pe_dev, bm_c, bm_h, 0, int(r0), int(r1), _vp(int(out)),
+                                        int(ld), 1, _vp(stream)))
+        return None
+
     def record_hits(self, rows: Sequence[int], voxels: Sequence[int], rotation: int = 0,
                     opts: Optional[PeOptions] = None) -> np.ndarray:
         """Per-ray hit records of entries (rows[i], voxels[i]); shape (n, rays, words)."""
@@ -252,6 +334,24 @@ def pe_compute_static(p, dst_ptr: int, ld: int, rotation: int = 0, rows: Optiona
     _check(lib().sm_pe_compute_static(_fptr(col), col.size, _fptr(det), det.size, _fptr(img), img.size,
                                       ctypes.byref(opts), int(rotation), int(r0), int(r1), int(z0), int(nz),
                                       _vp(int(dst_ptr)), int(ld), _vp(stream)))
+
+
+def scatter_legacy(parts: str, collimator, detector, image, physics, pe: np.ndarray, geo_crystal: Optional[str],
+                   geo_collimator: Optional[str], dst: np.ndarray, cuda_id: int = 0) -> int:
+    """The reference's ``scatter`` host entry points (combined, crystal-only,
+    collimator-only) through ``sm_scatter_legacy``; tables of at least
+    80000 / 80000 / 100 / 100 floats, host ``pe`` and ``dst`` of [N][V]."""
+    col = None if collimator is None else _as_f32(collimator)
+    det, img, phy = _as_f32(detector), _as_f32(image), _as_f32(physics)
+    pe_a = _as_f32(pe) if pe is not None else np.zeros(1, np.float32)
+    if not (dst.dtype == np.float32 and dst.flags.c_contiguous):
+        raise SysmatError(-1, "dst must be a C-contiguous float32 array")
+    rc = lib().sm_scatter_legacy(SCATTER_PARTS[parts], None if col is None else _fptr(col), _fptr(det), _fptr(img),
+                                 _fptr(phy), _fptr(pe_a), None if geo_crystal is None else geo_crystal.encode(),
+                                 None if geo_collimator is None else geo_collimator.encode(), _fptr(dst), int(cuda_id))
+    if rc < 0:
+        raise SysmatError(rc, (lib().sm_last_error() or b"").decode(errors="replace"))
+    return rc
 
 
 def primitive_batch(kind: str, args: np.ndarray) -> np.ndarray:

@@ -161,11 +161,26 @@ def two_plates_small(seed: int = 3) -> Params:
     return Params(col, det, img, build_physics(), sv=(2, 2, 2), sc=(2, 4, 2), name="two_plates_small")
 
 
+def scatter_mid(seed: int = 5, same_window: int = 1) -> Params:
+    """2 layers of 8x8 crystals behind one plate of 5x5 jittered holes; 8x8x6
+    voxels of 1.5 mm.  Small enough for the CPU oracle over the full matrix."""
+    rng = np.random.default_rng(seed)
+    holes = grid_holes(5, 5, 5.0, lambda: float(rng.uniform(0.5, 0.8)), 4.0, 0.0, jitter=0.6, rng=rng)
+    col = build_collimator([_plate(40.0, 4.0, 40.0, 0.0, holes)])
+    crystals = crystal_layer(8, 8, 2.0, (2.0, 5.0, 2.0), 14.0, CZT)
+    crystals += crystal_layer(8, 8, 2.0, (2.0, 5.0, 2.0), 19.5, CZT)
+    det = build_detector(crystals)
+    img = build_image((8, 8, 6), (1.5, 1.5, 1.5), fov_to_plate0=20.0)
+    return Params(col, det, img, build_physics(same_window=same_window), sv=(1, 1, 1), sc=(2, 4, 2),
+                  name="scatter_mid")
+
+
 NAMED = {
     "pe_small": pe_small,
     "pe_large": pe_large,
     "scatter_small": scatter_small,
     "scatter_large": scatter_large,
+    "scatter_mid": scatter_mid,
     "tiny": tiny,
     "two_plates_small": two_plates_small,
 }

@@ -50,9 +50,11 @@ int PESysMatGen(float* parameter_Collimator, float* parameter_Detector, float* p
  * [N][V].  Physics[8] / Physics[9] == 1 compute the geometry bitmaps and write
  * them to FnameGeoCrystal / FnameGeoCollimator, otherwise they are read from
  * those files.  Returns V, or -1 on failure. */
+#ifndef SYSMAT_B200_SINGLE_PART_SCATTER   /* defined by the two single-part shim libraries */
 int scatter(float* parameter_Collimator, float* parameter_Detector, float* parameter_Image,
             float* parameter_Physics, float* PE_SysMat, const char* FnameGeoCrystal,
             const char* FnameGeoCollimator, float* dst, int cuda_id);
+#endif
 
 /* ---- status codes ---------------------------------------------------------- */
 enum {
@@ -150,6 +152,56 @@ int sm_pe_record_hits(sm_context* ctx, const sm_geometry* geo, const sm_pe_optio
  * (costs a little time and synchronises the call). */
 int sm_pe_set_counters(sm_context* ctx, int enable);
 int sm_pe_last_counters(sm_context* ctx, int64_t out[4]);
+
+/* ---- primary-Compton scatter sysmat ------------------------------------------ */
+typedef struct sm_scatter_options {
+    int sp[3];   /* scatter points per scatter crystal (x, y = depth, z): sub-cell centres of
+                    the crystal, each with an equal share of its Compton probability;
+                    1 x 1 x 1 = the crystal centre, as the reference                        */
+    int parts;   /* 1: scatter in the crystals, 2: in the plate-0 holes, 3: both (summed)    */
+    int flags;   /* reserved, 0                                                              */
+} sm_scatter_options;
+
+/* Reference mode: sp = 1 x 1 x 1, both parts (ScatterGen_RayTracing_CircularHole). */
+void sm_scatter_options_reference(sm_scatter_options* opt);
+
+/* Sizes in uint32 words of the geometry-relationship bitmaps, in the
+ * reference's file format (scatter.cu:2053-2056, :2224-2229): out[0] crystal
+ * bitmap (N (N + 1) / 2 pairs x N bits), out[1] collimator bitmap (H0 x N x N
+ * bits, H0 = holes of plate 0). */
+int sm_scatter_bitmap_words(const sm_geometry* geo, int64_t out[2]);
+
+/* Computes either bitmap (NULL skips it) into device (on_device != 0, async on
+ * `stream`) or host buffers, bit for bit the reference's
+ * geometryRelationShip_Crystal2Crystal / _Collimator2Crystal
+ * (scatter.cu:1440-1540, :1939-2009). */
+int sm_scatter_bitmaps(sm_context* ctx, const sm_geometry* geo, uint32_t* crystal, uint32_t* collimator,
+                       int on_device, void* stream);
+
+/* Primary-Compton scatter sysmat of rotation `rotation` for detector rows
+ * [row0, row1) and every voxel: dst[(r - row0) * ld + v].  Replaces the
+ * kernels crystalScatterSysMatCuda / collimatorScatterSysMatCuda
+ * (scatter.cu:1077-1437, :1544-1936).  pe: that rotation's PE sysmat
+ * [N][ld_pe] (needed for parts & 1; device when pe_on_device).  Bitmaps:
+ * NULL = computed here; else device (bitmaps_on_device) or host words as
+ * read from the reference's files.  dst on the device makes the call
+ * asynchronous on `stream` when its inputs are on the device too. */
+int sm_scatter_compute(sm_context* ctx, const sm_geometry* geo, const sm_scatter_options* opt, int rotation,
+                       const float* pe, int64_t ld_pe, int pe_on_device, const uint32_t* crystal_bitmap,
+                       const uint32_t* collimator_bitmap, int bitmaps_on_device, int row0, int row1, float* dst,
+                       int64_t ld, int dst_on_device, void* stream);
+
+/* The reference's three `scatter` host entry points in one:
+ *   parts 3: ScatterGen_RayTracing_CircularHole/scatter.h:4-5 (geo_crystal, geo_collimator)
+ *   parts 1: ScatterGen_Crystal/scatter.h:4 (collimator table may be NULL; geo_crystal)
+ *   parts 2: ScatterGen_Collimator/scatter.h:4-5 (geo_collimator)
+ * Host tables of 80000 / 80000 / 100 / 100 floats, PE_SysMat = [N][V] host
+ * (the rotation Image[20] selects the image rotation), dst = [N][V] host.
+ * Physics[8] / Physics[9] == 1 compute the bitmaps and write them to the
+ * files, otherwise the files are read.  Returns V or a negative SM_ERR_*. */
+int sm_scatter_legacy(int parts, float* parameter_Collimator, float* parameter_Detector, float* parameter_Image,
+                      float* parameter_Physics, float* PE_SysMat, const char* geo_crystal,
+                      const char* geo_collimator, float* dst, int cuda_id);
 
 /* Diagnostic: evaluate the tracer's ray primitives on the current device for
  * n argument rows (host arrays).  kind 0: chord through a box (12 floats:

@@ -186,3 +186,130 @@ def primitive(kind: str, args: np.ndarray, impl: str = "oracle") -> np.ndarray:
     if impl == "dual":
         return _batch(getattr(oracle_lib(), "oracle_" + name + "_dual"), args, width)
     return _batch(getattr(ref_lib("pe_f32"), "ref_" + name), args, width)
+
+
+# ---------------------------------------------------------------------------
+# Primary-Compton scatter (oracle_scatter.cpp and the reference's scatter.cu)
+# ---------------------------------------------------------------------------
+
+_u32p = ctypes.POINTER(ctypes.c_uint32)
+
+
+def crystal_bitmap_words(n_crystals: int) -> int:
+    """uint32 words of the crystal bitmap: N(N+1)/2 pairs x N bits (scatter.cu:2053-2056)."""
+    bits = (n_crystals * (n_crystals + 1) // 2) * n_crystals
+    return (bits + 31) // 32
+
+
+def collimator_bitmap_words(n_crystals: int, n_holes0: int) -> int:
+    bits = n_holes0 * n_crystals * n_crystals
+    return (bits + 31) // 32
+
+
+def layer0_holes(params) -> int:
+    return int(np.floor(np.float32(params.collimator[10]) + np.float32(0.01)))
+
+
+def oracle_bitmap_crystal(params) -> np.ndarray:
+    det = np.ascontiguousarray(params.detector, dtype=np.float32)
+    n = crystal_bitmap_words(params.n_crystals)
+    out = np.zeros(n, dtype=np.uint32)
+    oracle_lib().oracle_bitmap_crystal(_ptr(det, _f32p), ctypes.c_longlong(det.size), _ptr(out, _u32p),
+                                       ctypes.c_longlong(n))
+    return out
+
+
+def oracle_bitmap_collimator(params) -> np.ndarray:
+    det = np.ascontiguousarray(params.detector, dtype=np.float32)
+    col = np.ascontiguousarray(params.collimator, dtype=np.float32)
+    n = collimator_bitmap_words(params.n_crystals, layer0_holes(params))
+    out = np.zeros(n, dtype=np.uint32)
+    oracle_lib().oracle_bitmap_collimator(_ptr(det, _f32p), ctypes.c_longlong(det.size), _ptr(col, _f32p),
+                                          ctypes.c_longlong(col.size), _ptr(out, _u32p), ctypes.c_longlong(n))
+    return out
+
+
+def _scatter_tables(params, rotation):
+    col = np.ascontiguousarray(params.collimator, dtype=np.float32)
+    det = np.ascontiguousarray(params.detector, dtype=np.float32)
+    img = np.zeros(100, np.float32)
+    img[:min(100, params.image.size)] = params.image[:100]
+    img[20] = np.float32(rotation)
+    phy = np.zeros(100, np.float32)
+    phy[:min(100, params.physics.size)] = params.physics[:100]
+    return col, det, img, phy
+
+
+def oracle_scatter_entries(params, kind: str, rows, voxels, bitmap: np.ndarray, pe: Optional[np.ndarray] = None,
+                           sp=(1, 1, 1), mode: str = "fp64", rotation: int = 0, nthreads: int = 0) -> np.ndarray:
+    """Scatter sysmat entries from the restatement.  kind 'crystal' needs the
+    [N][V] float32 PE matrix ``pe``; ``sp`` = scatter points per crystal."""
+    col, det, img, phy = _scatter_tables(params, rotation)
+    rows = np.ascontiguousarray(rows, dtype=np.int64)
+    vox = np.ascontiguousarray(voxels, dtype=np.int64)
+    out = np.zeros(rows.size, dtype=np.float64)
+    k = 0 if kind == "crystal" else 1
+    if pe is None:
+        pe = np.zeros(1, np.float32)
+    pe = np.ascontiguousarray(pe, dtype=np.float32)
+    bm = np.ascontiguousarray(bitmap, dtype=np.uint32)
+    spa = np.asarray(sp, dtype=np.int32)
+    oracle_lib().oracle_scatter_entries(ctypes.c_int(k), _ptr(col, _f32p), _ptr(det, _f32p), _ptr(img, _f32p),
+                                        _ptr(phy, _f32p), _ptr(pe, _f32p), _ptr(bm, _u32p), _ptr(spa, _i32p),
+                                        _ptr(rows, _i64p), _ptr(vox, _i64p), ctypes.c_longlong(rows.size),
+                                        ctypes.c_int(0 if mode == "fp32" else 1), _ptr(out, _f64p),
+                                        ctypes.c_int(nthreads))
+    return out
+
+
+def oracle_compton_integral(args: np.ndarray, mode: str = "fp64") -> np.ndarray:
+    a = np.ascontiguousarray(args, dtype=np.float32).reshape(-1, 3)
+    out = np.zeros(a.shape[0], dtype=np.float64)
+    oracle_lib().oracle_compton_integral_batch(_ptr(a, _f32p), ctypes.c_longlong(a.shape[0]),
+                                               ctypes.c_int(0 if mode == "fp32" else 1), _ptr(out, _f64p))
+    return out
+
+
+def ref_bitmap_crystal(params) -> np.ndarray:
+    lib = ref_lib("scatter_f32")
+    det = np.ascontiguousarray(params.detector, dtype=np.float32)
+    out = np.zeros(crystal_bitmap_words(params.n_crystals), dtype=np.uint32)
+    lib.ref_bitmap_crystal(_ptr(det, _f32p), ctypes.c_int64(det.size), _ptr(out, _u32p))
+    return out
+
+
+def ref_bitmap_collimator(params) -> np.ndarray:
+    lib = ref_lib("scatter_f32")
+    det = np.ascontiguousarray(params.detector, dtype=np.float32)
+    col = np.ascontiguousarray(params.collimator, dtype=np.float32)
+    out = np.zeros(collimator_bitmap_words(params.n_crystals, layer0_holes(params)), dtype=np.uint32)
+    lib.ref_bitmap_collimator(_ptr(det, _f32p), ctypes.c_int64(det.size), _ptr(col, _f32p), ctypes.c_int64(col.size),
+                              _ptr(out, _u32p))
+    return out
+
+
+def ref_scatter_entries(params, kind: str, rows, voxels, bitmap: np.ndarray, pe: Optional[np.ndarray] = None,
+                        variant: str = "f32", rotation: int = 0, nthreads: int = 0) -> np.ndarray:
+    """Entries computed by the reference's own scatter kernel code on the host."""
+    lib = ref_lib("scatter_" + variant)
+    col, det, img, phy = _scatter_tables(params, rotation)
+    rows = np.ascontiguousarray(rows, dtype=np.int64)
+    vox = np.ascontiguousarray(voxels, dtype=np.int64)
+    out = np.zeros(rows.size, dtype=np.float64)
+    bm = np.ascontiguousarray(bitmap, dtype=np.uint32)
+    if kind == "crystal":
+        pe = np.ascontiguousarray(pe, dtype=np.float32)
+        lib.ref_crystal_scatter_entries(_ptr(det, _f32p), ctypes.c_int64(det.size), _ptr(img, _f32p),
+                                        _ptr(phy, _f32p), _ptr(pe, _f32p), _ptr(bm, _u32p), _ptr(rows, _i64p),
+                                        _ptr(vox, _i64p), ctypes.c_int64(rows.size), _ptr(out, _f64p),
+                                        ctypes.c_int(nthreads))
+    else:
+        lib.ref_collimator_scatter_entries(_ptr(col, _f32p), ctypes.c_int64(col.size), _ptr(det, _f32p),
+                                           ctypes.c_int64(det.size), _ptr(img, _f32p), _ptr(phy, _f32p),
+                                           _ptr(bm, _u32p), _ptr(rows, _i64p), _ptr(vox, _i64p),
+                                           ctypes.c_int64(rows.size), _ptr(out, _f64p), ctypes.c_int(nthreads))
+    return out
+
+
+def ref_compton_integral(args: np.ndarray, variant: str = "f32") -> np.ndarray:
+    return _batch(ref_lib("scatter_" + variant).ref_compton_integral_batch, args, 3)

@@ -37,8 +37,11 @@ extern thread_local ref_uint3 blockDim;
 extern thread_local unsigned int ref_div[3];
 
 /* One host thread evaluates one (row, col[, slice]) cell at a time, so the
- * device atomics become plain read-modify-writes in loop order. */
-template <class T> inline T atomicAdd(T* p, T v) { T old = *p; *p = old + v; return old; }
+ * device atomics become plain read-modify-writes in loop order.  As with
+ * CUDA's atomicAdd(float*, float), the value is first converted to the
+ * target's type (the scatter kernels pass a double expression,
+ * scatter.cu:1427, :1924). */
+template <class T, class U> inline T atomicAdd(T* p, U v) { T old = *p; *p = old + (T)v; return old; }
 inline unsigned int atomicOr(unsigned int* p, unsigned int v) { unsigned int old = *p; *p = old | v; return old; }
 
 typedef int cudaError_t;

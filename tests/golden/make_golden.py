@@ -9,7 +9,11 @@ small seeded geometries, and stores inputs and outputs as .npz files:
                          single-precision (f32) and double (f64) results.
 * ``prim_<kind>.npz``   ray-primitive calls (random plus axis-aligned and
                          near-tangent rays) with the reference's f32 results.
-* ``scatter_<case>.npz`` scatter entries (added once the scatter oracle exists).
+* ``scatter_<case>.npz`` primary-Compton scatter: tables, the PE sysmat fed in
+                         (float32, from the PE oracle), the reference's bitmaps
+                         (crystal and collimator words), sampled (row, voxel)
+                         cells, and the reference's f32 and f64 crystal- and
+                         collimator-scatter values.
 
 Usage: ``python tests/golden/make_golden.py`` (needs oracle/_ref built).
 """
@@ -37,6 +41,50 @@ PE_CASES = {
     "two_plates": (lambda: configs.two_plates_small(), None, 64, (0,)),
     "pe_small": (lambda: configs.pe_small(), None, 24, (0,)),
 }
+
+
+SCATTER_CASES = {
+    # name: (params factory, rotation, sampled cells or None for the full matrix)
+    "tiny": (lambda: configs.tiny(), 0, None),
+    "tiny_rot": (lambda: _per_crystal_window(configs.tiny(seed=4, rotated=True)), 1, None),
+    "mid": (lambda: configs.scatter_mid(), 0, 768),
+}
+
+
+def _per_crystal_window(p):
+    """Windows from each crystal's energy resolution (Physics[4] = 0)."""
+    p = p.copy()
+    p.physics = p.physics.copy()
+    p.physics[4] = 0.0
+    return p
+
+
+def scatter_fixture(name, factory, rotation, n_cells):
+    p = factory()
+    p.sv, p.sc = (1, 1, 1), (2, 4, 2)
+    N, V = p.n_crystals, p.n_voxels
+    rows = np.repeat(np.arange(N), V)
+    vox = np.tile(np.arange(V), N)
+    pe = oracle_py.oracle_pe_entries(p, rows, vox, "fp64", rotation=rotation).astype(np.float32).reshape(N, V)
+    bm_c = oracle_py.ref_bitmap_crystal(p)
+    bm_h = oracle_py.ref_bitmap_collimator(p)
+    if n_cells is not None:
+        rng = np.random.default_rng(zlib.crc32(("scatter_" + name).encode()))
+        pick = rng.choice(N * V, n_cells, replace=False)
+        rows, vox = rows[pick], vox[pick]
+    out = {}
+    for kind in ("crystal", "collimator"):
+        bm = bm_c if kind == "crystal" else bm_h
+        for variant in ("f32", "f64"):
+            out["%s_%s" % (kind, variant)] = oracle_py.ref_scatter_entries(p, kind, rows, vox, bm, pe, variant,
+                                                                           rotation=rotation)
+    np.savez_compressed(os.path.join(HERE, "scatter_%s.npz" % name),
+                        collimator=p.collimator[:100 + 9 * p.n_holes], detector=p.detector[:1 + 12 * N],
+                        image=p.image, physics=p.physics, rotation=np.int64(rotation), pe=pe,
+                        bitmap_crystal=bm_c, bitmap_collimator=bm_h, rows=rows, voxels=vox,
+                        **{"ref_" + k: v for k, v in out.items()})
+    print("scatter_%s: %d cells, nonzero crystal %d collimator %d" % (
+        name, rows.size, int((out["crystal_f64"] != 0).sum()), int((out["collimator_f64"] != 0).sum())))
 
 
 def prim_rays(kind: str, n: int, seed: int) -> np.ndarray:
@@ -80,6 +128,10 @@ def prim_rays(kind: str, n: int, seed: int) -> np.ndarray:
 
 
 def main():
+    if len(sys.argv) > 1 and sys.argv[1] == "scatter":
+        for name, (factory, rotation, n_cells) in SCATTER_CASES.items():
+            scatter_fixture(name, factory, rotation, n_cells)
+        return
     if not oracle_py.ref_available("pe_f32"):
         raise SystemExit("oracle/_ref/libref_pe_f32.so missing: run `make -C oracle ref` first")
     for name, (factory, override, n, rotations) in PE_CASES.items():
@@ -102,6 +154,9 @@ def main():
                             rotation=np.concatenate(rot_all), ref_f32=np.concatenate(f32_all),
                             ref_f64=np.concatenate(f64_all))
         print("pe_%s: %d cells, nonzero %d" % (name, len(np.concatenate(f32_all)), int((np.concatenate(f32_all) != 0).sum())))
+    if oracle_py.ref_available("scatter_f32"):
+        for name, (factory, rotation, n_cells) in SCATTER_CASES.items():
+            scatter_fixture(name, factory, rotation, n_cells)
     for kind, seed in (("box", 11), ("inside", 12), ("cylinder", 13)):
         args = prim_rays(kind, 3000, seed)
         out = oracle_py.primitive(kind, args, impl="ref")

@@ -27,3 +27,15 @@ def rel_err(a, b, floor=0.0):
     if not nz.any():
         return np.zeros(0)
     return np.abs(a[nz] - b[nz]) / np.abs(b[nz])
+
+
+def load_scatter_golden(name: str):
+    """Params and arrays of tests/golden/scatter_<name>.npz."""
+    z = np.load(os.path.join(GOLDEN, "scatter_%s.npz" % name))
+    col = np.zeros(max(80000, z["collimator"].size), np.float32)
+    col[:z["collimator"].size] = z["collimator"]
+    det = np.zeros(max(80000, z["detector"].size), np.float32)
+    det[:z["detector"].size] = z["detector"]
+    p = Params(col, det, z["image"].astype(np.float32), z["physics"].astype(np.float32), (1, 1, 1), (2, 4, 2),
+               "scatter_" + name)
+    return p, z
