@@ -389,12 +389,98 @@ def run_ours(args, world, rank, local):
                 line["ref_cuda"] = {"unavailable": "%s" % exc}
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_reference_rate(p, args.cpu_seconds)
+        if world == 1 and args.scatter_steps > 0:
+            line["scatter"] = run_scatter(args, ctx, dev)
         print(json.dumps(line))
     geo.close()
     ctx.close()
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# Exact primary-Compton scatter (scatter_small: 2048 x 16384)
+# ---------------------------------------------------------------------------
+
+def ref_cuda_scatter_rate(p, d_pe, bitmaps, n_rows: int = 16):
+    """The reference's crystalScatterSysMatCuda / collimatorScatterSysMatCuda
+    (built for sm_100a) on the first n_rows detector rows, with the reference's
+    own launch shape; seconds per full matrix extrapolated by rows."""
+    import torch
+    path = os.path.join(ROOT, "oracle", "_ref", "libref_scatter_cuda.so")
+    if not os.path.exists(path):
+        return {"unavailable": "oracle/_ref/libref_scatter_cuda.so not built"}
+    lib = ctypes.CDLL(path)
+    N, V = p.n_crystals, p.n_voxels
+    pad = lambda a, n: np.pad(a.astype(np.float32), (0, max(0, n - a.size)))  # noqa: E731
+    dev = d_pe.device
+    det = torch.from_numpy(pad(p.detector, 80000)).to(dev)
+    col = torch.from_numpy(pad(p.collimator, 80000)).to(dev)
+    img = torch.from_numpy(p.image.astype(np.float32).copy()).to(dev)
+    phy = torch.from_numpy(p.physics.astype(np.float32).copy()).to(dev)
+    bc = torch.from_numpy(bitmaps[0].view(np.int32)).to(dev)
+    bh = torch.from_numpy(bitmaps[1].view(np.int32)).to(dev)
+    rows16 = (n_rows + 15) // 16 * 16
+    dst = torch.zeros((rows16, V), dtype=torch.float32, device=dev)
+    vp = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+    ms_c, ms_h = ctypes.c_float(0), ctypes.c_float(0)
+    h0 = int(np.floor(np.float32(p.collimator[10]) + np.float32(0.01)))
+    rc = lib.ref_cuda_crystal_scatter(vp(dst), vp(det), vp(img), vp(phy), vp(d_pe), vp(bc), N, V, n_rows, ctypes.byref(ms_c))
+    rc |= lib.ref_cuda_collimator_scatter(vp(dst), vp(col), vp(det), vp(img), vp(phy), vp(bh), N, V, h0, n_rows,
+                                          ctypes.byref(ms_h))
+    if rc != 0:
+        return {"unavailable": "reference scatter kernel returned CUDA error %d" % rc}
+    full_s = (ms_c.value + ms_h.value) / 1e3 * N / n_rows
+    return {"seconds_full_matrix": full_s, "entries_per_s": N * V / full_s, "sample_rows": n_rows,
+            "crystal_ms": ms_c.value, "collimator_ms": ms_h.value, "scatter_points": [1, 1, 1],
+            "note": "reference kernels scatter from crystal centres only (1 point per crystal)"}
+
+
+def run_scatter(args, ctx, dev):
+    """Exact crystal + collimator scatter of the scatter workload on the device
+    (PE sysmat resident in HBM), timed with CUDA events on the launch stream."""
+    import torch
+    import sysmat_b200
+    p = pe_workload("scatter_small")
+    g = sysmat_b200.Geometry(ctx, p)
+    N, V = p.n_crystals, p.n_voxels
+    stream = torch.cuda.Stream(device=dev)
+    d_pe = torch.zeros((N, V), dtype=torch.float32, device=dev)
+    d_out = torch.zeros((N, V), dtype=torch.float32, device=dev)
+    sp = tuple(args.scatter_points)
+    with torch.cuda.stream(stream):
+        g.pe(opts=g.options(sv=(1, 1, 1), sc=(2, 4, 2)), out=d_pe.data_ptr(), stream=stream.cuda_stream)
+    stream.synchronize()
+    res = {}
+    for parts in ("crystal", "collimator"):
+        times = []
+        for i in range(1 + args.scatter_steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            with torch.cuda.stream(stream):
+                e0.record(stream)
+                g.scatter(pe=d_pe.data_ptr(), sp=sp, parts=parts, out=d_out.data_ptr(), stream=stream.cuda_stream)
+                e1.record(stream)
+            stream.synchronize()
+            if i > 0:
+                times.append(e0.elapsed_time(e1) / 1e3)
+        res[parts] = min(times)
+    total = res["crystal"] + res["collimator"]
+    bitmaps = g.scatter_bitmaps()
+    out = {"workload": "scatter_small: 32x32x16 voxels of 1 mm, pe_small collimator (49 holes), 2 layers of 32x32 "
+                       "crystals [2048 x 16384]; PE input from the tracer (voxel centres, 2x4x2 sub-cells)",
+           "scatter_points": list(sp), "crystal_s": res["crystal"], "collimator_s": res["collimator"],
+           "seconds": total, "entries_per_s": N * V / total,
+           "terms_per_s": N * (N - 1) * V * int(np.prod(sp)) / res["crystal"],
+           "timed": "bitmaps + pair sums + main kernel per call, device-resident PE, CUDA events, best of %d"
+                    % args.scatter_steps}
+    if not args.no_ref_cuda:
+        try:
+            out["ref_cuda"] = ref_cuda_scatter_rate(p, d_pe, bitmaps)
+        except Exception as exc:  # the reference kernel is a baseline, not the product
+            out["ref_cuda"] = {"unavailable": str(exc)}
+    g.close()
+    return out
 
 
 def main():
@@ -411,6 +497,8 @@ def main():
     ap.add_argument("--row0", type=int, default=0, help="first crystal row when --rows limits them")
     ap.add_argument("--no-ref-cuda", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--scatter-steps", type=int, default=1, help="timed runs of the exact scatter (0 skips it)")
+    ap.add_argument("--scatter-points", type=int, nargs=3, default=[2, 4, 2])
     args = ap.parse_args()
     world, rank, local = dist_setup()
     if args.impl == "reference":

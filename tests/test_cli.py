@@ -1,0 +1,76 @@
+"""The command-line generators (gpu-spect-pet-sysmat_b200/bin/), run as the
+reference's CLIs are run: Params_*.dat in the working directory, the same
+flags, the same output files and layout ([rotation][crystal][voxel] float32)."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import sysmat_b200
+from sysmat_b200 import configs
+
+BIN = os.path.abspath(os.path.join(os.path.dirname(sysmat_b200.__file__), "..", "bin"))
+
+
+def run(tool, args, cwd):
+    return subprocess.run([os.path.join(BIN, tool)] + list(args), cwd=cwd, capture_output=True, text=True, timeout=600)
+
+
+def shift_name(prefix, p):
+    return "%s_shift_%f_%f_%f.sysmat" % (prefix, p.image[8], p.image[9], p.image[10])
+
+
+@pytest.mark.parametrize("tool", ["PEGen_CircularHole", "ScatterGen_CircularHole", "ScatterGen_Crystal",
+                                  "ScatterGen_Collimator"])
+def test_help_and_unknown_flags(tool, tmp_path):
+    configs.tiny().write_dat(str(tmp_path))
+    r = run(tool, ["-h"], tmp_path)
+    assert r.returncode == 0 and "Usage" in r.stdout
+    r = run(tool, ["-bogus"], tmp_path)
+    assert r.returncode != 0 and "Unknown parameter" in r.stderr
+
+
+def test_missing_params_file_is_reported(tmp_path):
+    r = run("PEGen_CircularHole", [], tmp_path)
+    assert r.returncode != 0 and "Params_Collimator.dat" in r.stderr
+
+
+@pytest.mark.gpu
+def test_pegen_and_scattergen_files(tmp_path):
+    p = configs.tiny(seed=4, rotated=True)          # 2 rotations, rotated crystals, shifted FOV
+    p.write_dat(str(tmp_path))
+    r = run("PEGen_CircularHole", ["-cuda", "0"], tmp_path)
+    assert r.returncode == 0, r.stderr
+    N, V = p.n_crystals, p.n_voxels
+    pe = np.fromfile(tmp_path / shift_name("PE_SysMat", p), np.float32).reshape(2, N, V)
+    ctx = sysmat_b200.Context(0)
+    g = sysmat_b200.Geometry(ctx, p)
+    ref_opts = sysmat_b200.PeOptions.make((1, 1, 1), (8, 16, 8))
+    for rot in range(2):
+        assert np.array_equal(pe[rot], g.pe(rotation=rot, opts=ref_opts))
+    # combined scatter generator: computes and writes the bitmaps, then the sysmats
+    r = run("ScatterGen_CircularHole", [], tmp_path)
+    assert r.returncode == 0, r.stderr
+    sc = np.fromfile(tmp_path / shift_name("Scatter_SysMat", p), np.float32).reshape(2, N, V)
+    full = np.fromfile(tmp_path / shift_name("SysMat_withScatter", p), np.float32).reshape(2, N, V)
+    for rot in range(2):
+        assert np.array_equal(sc[rot], g.scatter(pe=pe[rot], rotation=rot))
+    assert np.array_equal(full, pe + sc)
+    assert (tmp_path / "GeometryRelationShip_Crystal2Crystal").exists()
+    # reading the bitmaps back gives the same matrix
+    os.rename(tmp_path / "GeometryRelationShip_Crystal2Crystal", tmp_path / "gc")
+    os.rename(tmp_path / "GeometryRelationShip_Collimator2Crystal", tmp_path / "gh")
+    os.remove(tmp_path / shift_name("Scatter_SysMat", p))
+    r = run("ScatterGen_CircularHole", ["-GeoCrystal", "gc", "-GeoCollimator", "gh"], tmp_path)
+    assert r.returncode == 0, r.stderr
+    assert np.array_equal(np.fromfile(tmp_path / shift_name("Scatter_SysMat", p), np.float32).reshape(2, N, V), sc)
+    # single-part generators
+    r1 = run("ScatterGen_Crystal", ["-GeoCrystal", "gc"], tmp_path)
+    r2 = run("ScatterGen_Collimator", ["-GeoCollimator", "gh"], tmp_path)
+    assert r1.returncode == 0 and r2.returncode == 0, r1.stderr + r2.stderr
+    c = np.fromfile(tmp_path / shift_name("Scatter_Crystal_SysMat", p), np.float32).reshape(2, N, V)
+    h = np.fromfile(tmp_path / shift_name("Scatter_SysMat", p), np.float32).reshape(2, N, V)
+    np.testing.assert_allclose(sc, c.astype(np.float64) + h, rtol=1e-6, atol=0)
+    g.close()
+    ctx.close()
