@@ -280,6 +280,7 @@ __global__ void __launch_bounds__(kScThreads, 2) scatter_main_kernel(ScatterPara
             D.hi = (1.0f + D.res / 2.0f) * P.e0;
         }
         D.on = P.use_compton == 1 && pos.w > 0.01f;   // (scatter.cu:1203-1205)
+        D.c_cut = window_cos_cut(P.e0, P.alpha, D.res, D.lo);
         scale = KIND == kScatterCrystal ? D.mu_c / D.mu_pe / (float)T.n_points : P.plate_c_over_t;
     }
     if (warp == 0) S.scale[lane] = scale;
@@ -287,6 +288,10 @@ __global__ void __launch_bounds__(kScThreads, 2) scatter_main_kernel(ScatterPara
 
     const int x = x0 + warp;
     const float inv_norm = T.kn_inv_norm;
+    // this warp's voxel column: I0 + t e, t in [0, col_t] (image y axis, rotated)
+    const float4 col0 = S.vox[warp][0];
+    const float col_ex = -P.sin_a, col_ey = P.cos_a;
+    const float col_t = (float)(min(kScBrickY, P.ny - y0) - 1) * P.vy;
     if (KIND == kScatterCrystal) {
         const uint32_t* srcw = P.brick_sources + (long long)b * P.src_words;
         for (int wd = 0; wd < P.src_words; ++wd) {
@@ -310,9 +315,14 @@ __global__ void __launch_bounds__(kScThreads, 2) scatter_main_kernel(ScatterPara
                     const int q = s * T.n_points + p;
                     const float4 src = T.crystal_src[q];
                     Src C;
-                    const float4 pr = D.on ? P.pair[(long long)q * P.pair_ld + (d - P.pair_d0)] : make_float4(0.f, 0.f, 0.f, 0.f);
-                    make_src(D, src, pr, C);
-                    const bool on = D.on && s != d;
+                    bool on = D.on && s != d;
+                    if (on) {
+                        make_src_basic(D, src, C);
+                        // no voxel of the column passes the window cut: the lane sits out
+                        on = column_max_cos(C, col0.x, col0.y, col0.z, col_ex, col_ey, 0.0f, col_t) > D.c_cut;
+                    }
+                    if (!__any_sync(0xffffffffu, on)) continue;
+                    if (on) make_src_rest(D, P.pair[(long long)q * P.pair_ld + (d - P.pair_d0)], C);
                     unsigned m = live;
                     while (m) {
                         const int j = __ffs(m) - 1;
@@ -333,9 +343,13 @@ __global__ void __launch_bounds__(kScThreads, 2) scatter_main_kernel(ScatterPara
         for (int h = 0; h < T.n_holes0; ++h) {
             const float4 src = T.hole_src[h];
             Src C;
-            const float4 pr = D.on ? P.pair[(long long)h * P.pair_ld + (d - P.pair_d0)] : make_float4(0.f, 0.f, 0.f, 0.f);
-            make_src(D, src, pr, C);
-            if (!D.on || x >= P.nx) continue;
+            bool on = D.on && x < P.nx;
+            if (on) {
+                make_src_basic(D, src, C);
+                on = column_max_cos(C, col0.x, col0.y, col0.z, col_ex, col_ey, 0.0f, col_t) > D.c_cut;
+            }
+            if (!on) continue;
+            make_src_rest(D, P.pair[(long long)h * P.pair_ld + (d - P.pair_d0)], C);
             for (int j = 0; j < kScBrickY; ++j) {
                 const float4 I = S.vox[warp][j];
                 if (I.w < 0.0f) break;
