@@ -64,8 +64,12 @@ struct ScatterParams {
     float win_lo, win_hi;        // Physics[5], Physics[6]
     // collimator-scatter weight: mu_compton / mu_total of plate 0 (Collimator[17] / Collimator[15])
     float plate_c_over_t;
-    // rows [row0, row1) of detectors
-    int row0, row1;
+    // detectors: perm[r] for ranks r in [rank0, rank1); perm orders the requested
+    // rows so that 32 consecutive ranks are spatially close (depth layer, then a
+    // Morton curve over x, z); dst row of detector d is d - dst_row0
+    const int* perm;
+    int rank0, rank1;
+    int dst_row0;
     // bricks
     int bricks_x, bricks_y, n_bricks;
     // inputs
@@ -74,7 +78,7 @@ struct ScatterParams {
     const uint32_t* brick_sources;   // crystal kind: [n_bricks][ceil(N/32)] sources with PE != 0 in the brick
     int src_words;
     const float4* pair;          // [source point][pair_ld]: sum L mu_pe, sum L mu_c, self path, absorption chord
-    int pair_d0;                 // detector of pair column 0
+    int pair_r0;                 // rank of pair column 0
     long long pair_ld;
     // output
     float* dst;
@@ -99,9 +103,12 @@ int64_t collimator_bitmap_words(int n_crystals, int n_holes0);
 
 cudaError_t launch_bitmap_crystal(uint32_t* words, int64_t n_words, const ScatterTables& T, cudaStream_t s);
 cudaError_t launch_bitmap_collimator(uint32_t* words, int64_t n_words, const ScatterTables& T, cudaStream_t s);
-// pair[q][d - d0] for every source point q of `kind` and detectors d in [d0, d1).
+// pair[q][r - r0] for every source point q of `kind` and detectors perm[r], r in [r0, r1).
 cudaError_t launch_scatter_pairs(int kind, const DevGeometry& G, const ScatterTables& T, const uint32_t* bitmap,
-                                 int d0, int d1, float4* pair, cudaStream_t s);
+                                 const int* perm, int r0, int r1, float4* pair, cudaStream_t s);
+
+// Ranks of detectors [row0, row1) in spatial order (see ScatterParams::perm).
+std::vector<int> spatial_order(const HostGeometry& g, int row0, int row1);
 cudaError_t launch_brick_sources(const ScatterParams& P, const ScatterTables& T, uint32_t* brick_sources,
                                  cudaStream_t s);
 cudaError_t launch_scatter_main(const ScatterParams& P, const DevGeometry& G, const ScatterTables& T,

@@ -110,8 +110,13 @@ int scatter_device(sm_context* ctx, const sm_geometry* geo, const int sp[3], int
 
     ScatterParams P{};
     fill_common(g, 0, angle, &P);
-    P.row0 = row0;
-    P.row1 = row1;
+    const std::vector<int> order = spatial_order(g, row0, row1);
+    DevBuf perm;
+    SM_TRY(perm.alloc(sizeof(int) * order.size(), s, "detector order"));
+    SM_CUDA(cudaMemcpyAsync(perm.p, order.data(), sizeof(int) * order.size(), cudaMemcpyHostToDevice, s));
+    SM_CUDA(cudaStreamSynchronize(s));   // the host order is released on return
+    P.perm = static_cast<const int*>(perm.p);
+    P.dst_row0 = row0;
     P.dst = d_dst;
     P.ld = ld;
     P.pe = d_pe;
@@ -150,20 +155,20 @@ int scatter_device(sm_context* ctx, const sm_geometry* geo, const int sp[3], int
         const int n_src = kind == kScatterCrystal ? N * T.n_points : h0;
         int chunk = (int)std::max<size_t>(kScTileD, kPairBudget / (sizeof(float4) * (size_t)std::max(1, n_src)));
         chunk = std::max(kScTileD, chunk / kScTileD * kScTileD);
-        const size_t pb = sizeof(float4) * (size_t)n_src * (size_t)std::min(chunk, row1 - row0);
+        const int n_rank = row1 - row0;
+        const size_t pb = sizeof(float4) * (size_t)n_src * (size_t)std::min(chunk, n_rank);
         DevBuf pair;
         SM_TRY(pair.alloc(pb, s, "scatter pairs"));
-        for (int c0 = row0; c0 < row1; c0 += chunk) {
-            const int c1 = std::min(row1, c0 + chunk);
-            SM_CUDA(launch_scatter_pairs(kind, geo->dev.view, T, kind == kScatterCrystal ? bmc : bmh, c0, c1,
+        for (int c0 = 0; c0 < n_rank; c0 += chunk) {
+            const int c1 = std::min(n_rank, c0 + chunk);
+            SM_CUDA(launch_scatter_pairs(kind, geo->dev.view, T, kind == kScatterCrystal ? bmc : bmh, P.perm, c0, c1,
                                          static_cast<float4*>(pair.p), s));
             ScatterParams Q = P;
             Q.kind = kind;
-            Q.row0 = c0;
-            Q.row1 = c1;
-            Q.dst = d_dst + (int64_t)(c0 - row0) * ld;
+            Q.rank0 = c0;
+            Q.rank1 = c1;
             Q.pair = static_cast<const float4*>(pair.p);
-            Q.pair_d0 = c0;
+            Q.pair_r0 = c0;
             Q.pair_ld = c1 - c0;
             Q.accumulate = written ? 1 : 0;
             SM_CUDA(launch_scatter_main(Q, geo->dev.view, T, s));

@@ -4,6 +4,7 @@
 // Compiled with -ffp-contract=off: positions and radii must round as the
 // reference's single-precision expressions do (scatter.cu:1466-1511, :1961-1994,
 // :1211-1219, :1700-1702).
+#include <algorithm>
 #include <cmath>
 
 #include "common.h"
@@ -185,6 +186,55 @@ int build_scatter_tables(const HostGeometry& g, const int sp[3], HostScatterTabl
     }
     build_kn_table(g.physics[7], &T.kn, &T.kn_inv_norm);
     return SM_OK;
+}
+
+// Depth layers (crystal centres within a quarter of the thinnest crystal of
+// each other in y) first, then a Morton curve over x and z quantised by the
+// narrowest crystal, so that 32 consecutive ranks form a compact 2-D patch of
+// one layer.  Lanes of a warp are detectors; a patch makes the energy-window
+// cull and the scattered photon's path coherent across the warp.
+std::vector<int> spatial_order(const HostGeometry& g, int row0, int row1) {
+    const int n = row1 - row0;
+    std::vector<int> ids(n);
+    for (int i = 0; i < n; ++i) ids[i] = row0 + i;
+    if (n <= 1) return ids;
+    float tmin = 1e30f, wmin = 1e30f, xmin = 1e30f, zmin = 1e30f;
+    for (int d = row0; d < row1; ++d) {
+        const float* sz = &g.c_size[4 * (size_t)d];
+        const float* ps = &g.c_pos[4 * (size_t)d];
+        tmin = std::min(tmin, sz[1]);
+        wmin = std::min(wmin, std::min(sz[0], sz[2]));
+        xmin = std::min(xmin, ps[0]);
+        zmin = std::min(zmin, ps[2]);
+    }
+    std::vector<int> by_y = ids;
+    std::stable_sort(by_y.begin(), by_y.end(), [&](int a, int b) { return g.c_pos[4 * (size_t)a + 1] < g.c_pos[4 * (size_t)b + 1]; });
+    std::vector<long long> layer(g.n_crystals, 0);
+    long long lay = 0;
+    float prev = g.c_pos[4 * (size_t)by_y[0] + 1];
+    for (int d : by_y) {
+        const float y = g.c_pos[4 * (size_t)d + 1];
+        if (y - prev > 0.25f * tmin) ++lay;
+        prev = y;
+        layer[d] = lay;
+    }
+    auto spread = [](uint32_t v) {   // 16 bits -> even bit positions
+        uint64_t x = v & 0xffffu;
+        x = (x | (x << 8)) & 0x00ff00ffu;
+        x = (x | (x << 4)) & 0x0f0f0f0fu;
+        x = (x | (x << 2)) & 0x33333333u;
+        x = (x | (x << 1)) & 0x55555555u;
+        return x;
+    };
+    std::vector<uint64_t> key(g.n_crystals, 0);
+    for (int d = row0; d < row1; ++d) {
+        const float* ps = &g.c_pos[4 * (size_t)d];
+        const uint32_t ix = (uint32_t)std::min(65535.0f, std::max(0.0f, std::floor((ps[0] - xmin) / wmin + 0.5f)));
+        const uint32_t iz = (uint32_t)std::min(65535.0f, std::max(0.0f, std::floor((ps[2] - zmin) / wmin + 0.5f)));
+        key[d] = ((uint64_t)layer[d] << 32) | spread(ix) | (spread(iz) << 1);
+    }
+    std::stable_sort(ids.begin(), ids.end(), [&](int a, int b) { return key[a] < key[b]; });
+    return ids;
 }
 
 }  // namespace smb

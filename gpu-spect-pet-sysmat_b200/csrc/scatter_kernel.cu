@@ -135,12 +135,14 @@ __global__ void bitmap_collimator_kernel(uint32_t* words, long long n_words, Sca
 // The detector unit is the whole crystal (the reference's divide = 1), whose
 // centre is the crystal centre.
 template <int KIND>
-__global__ void scatter_pair_kernel(DevGeometry G, ScatterTables T, const uint32_t* __restrict__ bitmap, int d0,
-                                    int d1, float4* __restrict__ pair, int n_sources) {
+__global__ void scatter_pair_kernel(DevGeometry G, ScatterTables T, const uint32_t* __restrict__ bitmap,
+                                    const int* __restrict__ perm, int r0, int r1, float4* __restrict__ pair,
+                                    int n_sources) {
     const int N = T.n_crystals;
-    const int d = d0 + blockIdx.x * blockDim.x + threadIdx.x;
-    if (d >= d1) return;
-    const long long ld = d1 - d0;
+    const int r = r0 + blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= r1) return;
+    const int d = perm[r];
+    const long long ld = r1 - r0;
     const float4 Dp = G.c.pos[d], Dsz = G.c.size[d], Dr = G.c.rot[d];
     for (int q = blockIdx.y; q < n_sources; q += gridDim.y) {
         float4 S;
@@ -204,7 +206,7 @@ __global__ void scatter_pair_kernel(DevGeometry G, ScatterTables T, const uint32
             const float labs = chord_through(xs, ys, zs, xt, yt, zt, ub);
             out = make_float4(a_pe, a_c, l1 - l2, labs);
         }
-        pair[(long long)q * ld + (d - d0)] = out;
+        pair[(long long)q * ld + (r - r0)] = out;
     }
 }
 
@@ -264,9 +266,10 @@ __global__ void __launch_bounds__(kScThreads, 2) scatter_main_kernel(ScatterPara
         S.vox[xx][yy] = v;
     }
 
-    const int d = P.row0 + dt * kScTileD + lane;
+    const int rank = P.rank0 + dt * kScTileD + lane;
+    const int d = rank < P.rank1 ? P.perm[rank] : -1;
     Det D;
-    D.on = d < P.row1;
+    D.on = rank < P.rank1;
     float scale = 0.0f;
     if (D.on) {
         const float4 pos = G.c.pos[d], sz = G.c.size[d], rt = G.c.rot[d], ph = G.c.phys[d];
@@ -322,7 +325,7 @@ __global__ void __launch_bounds__(kScThreads, 2) scatter_main_kernel(ScatterPara
                         on = column_max_cos(C, col0.x, col0.y, col0.z, col_ex, col_ey, 0.0f, col_t) > D.c_cut;
                     }
                     if (!__any_sync(0xffffffffu, on)) continue;
-                    if (on) make_src_rest(D, P.pair[(long long)q * P.pair_ld + (d - P.pair_d0)], C);
+                    if (on) make_src_rest(D, P.pair[(long long)q * P.pair_ld + (rank - P.pair_r0)], C);
                     unsigned m = live;
                     while (m) {
                         const int j = __ffs(m) - 1;
@@ -349,7 +352,7 @@ __global__ void __launch_bounds__(kScThreads, 2) scatter_main_kernel(ScatterPara
                 on = column_max_cos(C, col0.x, col0.y, col0.z, col_ex, col_ey, 0.0f, col_t) > D.c_cut;
             }
             if (!on) continue;
-            make_src_rest(D, P.pair[(long long)h * P.pair_ld + (d - P.pair_d0)], C);
+            make_src_rest(D, P.pair[(long long)h * P.pair_ld + (rank - P.pair_r0)], C);
             for (int j = 0; j < kScBrickY; ++j) {
                 const float4 I = S.vox[warp][j];
                 if (I.w < 0.0f) break;
@@ -371,15 +374,15 @@ __global__ void __launch_bounds__(kScThreads, 2) scatter_main_kernel(ScatterPara
     __syncthreads();
 
     // write the tile: (detector, y, 8 x) with x fastest
-    const int n_rows = min(kScTileD, P.row1 - (P.row0 + dt * kScTileD));
+    const int n_rows = min(kScTileD, P.rank1 - (P.rank0 + dt * kScTileD));
     for (int i = tid; i < n_rows * kScBrickY * kScBrickX; i += kScThreads) {
         const int xx = i & 7, yy = (i >> 3) & 31, dl = i >> 8;
         const int xv = x0 + xx, yv = y0 + yy;
         if (xv >= P.nx || yv >= P.ny) continue;
-        const int dd = P.row0 + dt * kScTileD + dl;
+        const int dd = P.perm[P.rank0 + dt * kScTileD + dl];
         const float sc = S.scale[dl];
         const long long col = (long long)xv + (long long)P.nx * (yv + (long long)P.ny * bz);
-        float* out = P.dst + (long long)(dd - P.row0) * P.ld + col;
+        float* out = P.dst + (long long)(dd - P.dst_row0) * P.ld + col;
         const float v = (float)S.acc[xx][yy][dl] * sc;
         *out = P.accumulate ? *out + v : v;
     }
@@ -412,14 +415,14 @@ cudaError_t launch_bitmap_collimator(uint32_t* words, int64_t n_words, const Sca
 }
 
 cudaError_t launch_scatter_pairs(int kind, const DevGeometry& G, const ScatterTables& T, const uint32_t* bitmap,
-                                 int d0, int d1, float4* pair, cudaStream_t s) {
+                                 const int* perm, int r0, int r1, float4* pair, cudaStream_t s) {
     const int n_src = kind == kScatterCrystal ? T.n_crystals * T.n_points : T.n_holes0;
-    if (d1 <= d0 || n_src <= 0) return cudaSuccess;
-    dim3 grid((d1 - d0 + 127) / 128, std::min(n_src, 65535));
+    if (r1 <= r0 || n_src <= 0) return cudaSuccess;
+    dim3 grid((r1 - r0 + 127) / 128, std::min(n_src, 65535));
     if (kind == kScatterCrystal)
-        scatter_pair_kernel<kScatterCrystal><<<grid, 128, 0, s>>>(G, T, bitmap, d0, d1, pair, n_src);
+        scatter_pair_kernel<kScatterCrystal><<<grid, 128, 0, s>>>(G, T, bitmap, perm, r0, r1, pair, n_src);
     else
-        scatter_pair_kernel<kScatterCollimator><<<grid, 128, 0, s>>>(G, T, bitmap, d0, d1, pair, n_src);
+        scatter_pair_kernel<kScatterCollimator><<<grid, 128, 0, s>>>(G, T, bitmap, perm, r0, r1, pair, n_src);
     return cudaGetLastError();
 }
 
@@ -433,7 +436,7 @@ cudaError_t launch_brick_sources(const ScatterParams& P, const ScatterTables& T,
 cudaError_t launch_scatter_main(const ScatterParams& P, const DevGeometry& G, const ScatterTables& T,
                                 cudaStream_t s) {
     const size_t smem = sizeof(ScSmem);
-    const long long d_tiles = (P.row1 - P.row0 + kScTileD - 1) / kScTileD;
+    const long long d_tiles = (P.rank1 - P.rank0 + kScTileD - 1) / kScTileD;
     const long long blocks = d_tiles * P.n_bricks;
     if (blocks <= 0) return cudaSuccess;
     if (blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
