@@ -391,6 +391,8 @@ def run_ours(args, world, rank, local):
             line["cpu_baseline"] = cpu_reference_rate(p, args.cpu_seconds)
         if world == 1 and args.scatter_steps > 0:
             line["scatter"] = run_scatter(args, ctx, dev)
+        if world == 1 and args.sweep_steps > 0:
+            line["sweep"] = run_sweep(args, ctx, dev)
         print(json.dumps(line))
     geo.close()
     ctx.close()
@@ -483,14 +485,75 @@ def run_scatter(args, ctx, dev):
     return out
 
 
+# ---------------------------------------------------------------------------
+# Batched design sweep: 64 seeded geometries in one persistent graph launch
+# ---------------------------------------------------------------------------
+
+def run_sweep(args, ctx, dev):
+    import torch
+    import sysmat_b200
+    from sysmat_b200 import configs
+    params = configs.sweep()
+    geos = [sysmat_b200.Geometry(ctx, p) for p in params]
+    t0 = time.perf_counter()
+    opts = []
+    for g in geos:
+        tuned, _ = sysmat_b200.autotune(g)
+        opts.append(tuned)
+    tune_s = time.perf_counter() - t0
+    outs = [torch.empty((g.n_crystals, g.nx * g.ny * g.nz), dtype=torch.float32, device=dev) for g in geos]
+    entries = sum(o.numel() for o in outs)
+    rays = sum(o.numel() * int(np.prod(p.sv)) * int(np.prod(p.sc)) for o, p in zip(outs, params))
+    stream = torch.cuda.Stream(device=dev)
+    batch = sysmat_b200.PeBatch(ctx, geos, opts, [o.data_ptr() for o in outs], [o.shape[1] for o in outs])
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+        stream.synchronize()
+        return e0.elapsed_time(e1) / 1e3
+
+    batch.run(stream.cuda_stream)          # captures the graph
+    stream.synchronize()
+    t_batch = min(timed(lambda: batch.run(stream.cuda_stream)) for _ in range(args.sweep_steps))
+
+    def sequential():
+        for g, o, op in zip(geos, outs, opts):
+            g.pe(opts=op, out=o.data_ptr(), stream=stream.cuda_stream)
+    t_seq = min(timed(sequential) for _ in range(args.sweep_steps))
+
+    def sequential_default():
+        for g, o in zip(geos, outs):
+            g.pe(opts=g.options(), out=o.data_ptr(), stream=stream.cuda_stream)
+    t_default = min(timed(sequential_default) for _ in range(args.sweep_steps))
+    ctx.sync(stream.cuda_stream)
+    info = batch.info()
+    batch.close()
+    for g in geos:
+        g.close()
+    return {"workload": "64 seeded geometries (grids 16^3..48^3, 1-3 plates, 16-400 holes per plate, 16^2..48^2 "
+                        "crystals x 1-4 layers), whole PE sysmat of each, voxel centres x 2x4x2 sub-cells",
+            "entries": entries, "rays": rays, "output_gb": entries * 4 / 1e9,
+            "batched_s": t_batch, "batched_entries_per_s": entries / t_batch, "batched_rays_per_s": rays / t_batch,
+            "sequential_s": t_seq, "sequential_entries_per_s": entries / t_seq, "speedup": t_seq / t_batch,
+            "sequential_default_brick_s": t_default, "autotune_gain": t_default / t_seq,
+            "work_items": info["items"], "persistent_ctas": info["ctas"], "autotune_s": tune_s,
+            "bricks": sorted(set(tuple(o.tile_voxels) for o in opts)),
+            "timed": "one CUDA-graph launch of the persistent kernel vs 64 sm_pe_compute launches on one stream, "
+                     "same autotuned bricks, CUDA events, best of %d" % args.sweep_steps}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=8)
+    ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="pe_large")
-    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--ref-entries", type=int, default=4096)
     ap.add_argument("--rows", type=int, default=0, help="limit the crystal rows per step (profiling runs)")
@@ -499,6 +562,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--scatter-steps", type=int, default=1, help="timed runs of the exact scatter (0 skips it)")
     ap.add_argument("--scatter-points", type=int, nargs=3, default=[2, 4, 2])
+    ap.add_argument("--sweep-steps", type=int, default=1, help="timed runs of the batched sweep (0 skips it)")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     if args.impl == "reference":

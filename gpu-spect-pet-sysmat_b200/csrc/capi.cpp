@@ -57,7 +57,7 @@ int context_collect_status(sm_context* ctx, cudaStream_t stream) {
     return SM_OK;
 }
 
-static int validate_pe(const sm_geometry* geo, const sm_pe_options* opt, int row0, int row1, int z0, int nz) {
+int validate_pe(const sm_geometry* geo, const sm_pe_options* opt, int row0, int row1, int z0, int nz) {
     for (int a = 0; a < 3; ++a) {
         if (opt->sv[a] < 1 || opt->sv[a] > 64) return fail(SM_ERR_INVALID, "sv[%d] = %d must be in 1..64", a, opt->sv[a]);
         if (opt->sc[a] < 1 || opt->sc[a] > kMaxSubcellsPerAxis)
@@ -200,8 +200,10 @@ int sm_pe_compute(sm_context* ctx, const sm_geometry* geo, const sm_pe_options* 
     const int64_t slab = (int64_t)g.nx * g.ny * nz;
     if (ld < slab) return fail(SM_ERR_INVALID, "ld = %lld is smaller than the slab's %lld voxels", (long long)ld, (long long)slab);
     cudaStream_t stream = (cudaStream_t)stream_ptr;
+    sm_pe_options tuned = *opt;
+    if (opt->flags & SM_PE_AUTOTUNE) SM_TRY(sm_pe_autotune(ctx, geo, opt, rotation, &tuned, nullptr));
     PEParams P;
-    pe_plan(g, opt->sv, opt->sc, opt->tile_voxels, rotation, row0, row1, g.nz, z0, nz, &P);
+    pe_plan(g, tuned.sv, tuned.sc, tuned.tile_voxels, rotation, row0, row1, g.nz, z0, nz, &P);
     P.status = ctx->d_status;
     P.counters = ctx->collect_counters ? ctx->d_counters : nullptr;
     if (P.counters) SM_CUDA(cudaMemsetAsync(ctx->d_counters, 0, 4 * sizeof(unsigned long long), stream));

@@ -27,4 +27,5 @@ namespace smb {
 int context_bind(sm_context* ctx);
 int context_collect_status(sm_context* ctx, cudaStream_t stream);
 sm_context* legacy_context(int cuda_id);
+int validate_pe(const sm_geometry* geo, const sm_pe_options* opt, int row0, int row1, int z0, int nz);
 }  // namespace smb

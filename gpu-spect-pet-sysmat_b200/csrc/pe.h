@@ -11,13 +11,13 @@ namespace smb {
 
 constexpr int kPeWarps = 8;            // warps per CTA = crystals per tile
 constexpr int kPeThreads = 32 * kPeWarps;
-constexpr int kSupC = 512;             // tile superset capacity, crystals
-constexpr int kSupH = 256;             // tile superset capacity, holes
+constexpr int kSupC = 1024;            // tile superset capacity, crystals
+constexpr int kSupH = 384;             // tile superset capacity, holes
 constexpr int kMaxGroup = 4;           // voxel sub-points whose candidate masks are live at once
 constexpr int kMaxTileVoxels = 128;    // voxels per brick
-constexpr int kListC = 256;            // per-voxel candidate list capacity, crystals
+constexpr int kListC = 512;            // per-voxel candidate list capacity, crystals
 constexpr int kListH = 128;            // per-voxel candidate list capacity, holes
-constexpr int kMaxSubcellsPerAxis = 256;
+constexpr int kMaxSubcellsPerAxis = 64;
 constexpr int kRecHoles = 16;          // hit-record capacity per ray
 constexpr int kRecCrystals = 40;
 constexpr int kRecWords = 3 + kRecHoles + kRecCrystals;
@@ -68,5 +68,22 @@ void pe_plan(const HostGeometry& g, const int sv[3], const int sc[3], const int 
 cudaError_t pe_launch(const PEParams& p, const DevGeometry& geo, bool record, long long n_tiles, cudaStream_t stream);
 
 size_t pe_smem_bytes();
+
+// One geometry of a batch: its launch parameters, its tables, and the index
+// of its first work item; items [tile_begin, tile_begin + P.n_tiles).
+struct __align__(16) PeBatchGeom {
+    PEParams P;
+    DevGeometry G;
+    long long tile_begin;
+};
+
+constexpr int kBatchConst = 64;   // geometries per persistent launch (constant-memory table)
+
+// One persistent launch over `total` items of n_geoms <= kBatchConst
+// geometries (device table `geoms`, ordered by tile_begin, first item 0):
+// copies the table to constant memory, zeroes `counter`, launches.
+cudaError_t pe_batch_launch(const PeBatchGeom* geoms, int n_geoms, long long total, unsigned long long* counter,
+                            int grid, cudaStream_t stream);
+int pe_batch_blocks_per_sm();
 
 }  // namespace smb

@@ -428,13 +428,12 @@ __device__ __forceinline__ int warp_append(bool pass, int value, unsigned short*
     return count + __popc(bal);
 }
 
+// One tile (8 crystals x one voxel brick) of geometry G.  Shared by the
+// one-launch-per-geometry kernel and the persistent batch kernel.
 template <bool RECORD>
-__global__ void __launch_bounds__(kPeThreads, 2) pe_trace_kernel(PEParams P, DevGeometry G) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    PeSmem& S = *reinterpret_cast<PeSmem*>(smem_raw);
+__device__ __forceinline__ void pe_tile(const PEParams& P, const DevGeometry& G, PeSmem& S, long long tile) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 
-    const long long tile = P.tile_list ? P.tile_list[blockIdx.x] : (long long)blockIdx.x;
     const int ct = (int)(tile % P.n_ctiles);
     const long long vt = tile / P.n_ctiles;
     const int bxi = (int)(vt % P.tiles_x);
@@ -741,32 +740,105 @@ __global__ void __launch_bounds__(kPeThreads, 2) pe_trace_kernel(PEParams P, Dev
     }
 }
 
+template <bool RECORD>
+__global__ void __launch_bounds__(kPeThreads, 2) pe_trace_kernel(PEParams P, DevGeometry G) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    PeSmem& S = *reinterpret_cast<PeSmem*>(smem_raw);
+    const long long tile = P.tile_list ? P.tile_list[blockIdx.x] : (long long)blockIdx.x;
+    pe_tile<RECORD>(P, G, S, tile);
+}
+
+// The batch's geometries, in constant memory: the tile code reads launch
+// parameters in its inner loops, and constant-bank loads of a warp-uniform
+// index cost what kernel-parameter loads cost.  Written by the batch's own
+// graph (a device-to-device copy before each chunk's launch).
+__constant__ PeBatchGeom c_batch[kBatchConst];
+
+// Persistent kernel over the (geometry, tile) items of up to kBatchConst
+// geometries: each CTA takes the next item from a global counter until all
+// are done.  Geometries are laid out largest first, so the dynamic hand-out
+// balances the tail.  No CTA waits on another: the counter only hands out work.
+__global__ void __launch_bounds__(kPeThreads, 2) pe_batch_kernel(int n_geoms, long long total,
+                                                                 unsigned long long* counter) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    PeSmem& S = *reinterpret_cast<PeSmem*>(smem_raw);
+    __shared__ long long s_item;
+    __shared__ int s_geom;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            const long long item = (long long)atomicAdd(counter, 1ULL);
+            int lo = 0, hi = n_geoms - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (c_batch[mid].tile_begin <= item) lo = mid;
+                else hi = mid - 1;
+            }
+            s_item = item;
+            s_geom = lo;
+        }
+        __syncthreads();
+        const long long item = s_item;
+        const int g = s_geom;
+        if (item >= total) break;
+        pe_tile<false>(c_batch[g].P, c_batch[g].G, S, item - c_batch[g].tile_begin);
+        __syncthreads();
+    }
+}
+
 }  // namespace
 
 size_t pe_smem_bytes() { return sizeof(PeSmem); }
+
+// The dynamic shared memory limit is a per-device function attribute: set it
+// once per (device, kernel).
+static cudaError_t allow_smem(const void* fn, int which) {
+    static unsigned long long done[3] = {0, 0, 0};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 64 && (done[which] >> dev) & 1ULL) return cudaSuccess;
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(PeSmem));
+    if (e == cudaSuccess && dev < 64) done[which] |= 1ULL << dev;
+    return e;
+}
 
 cudaError_t pe_launch(const PEParams& p, const DevGeometry& geo, bool record, long long n_tiles, cudaStream_t stream) {
     const size_t smem = sizeof(PeSmem);
     if (n_tiles <= 0) return cudaSuccess;
     if (n_tiles > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
     if (record) {
-        static bool attr_set = false;
-        if (!attr_set) {
-            cudaError_t e = cudaFuncSetAttribute(pe_trace_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            if (e != cudaSuccess) return e;
-            attr_set = true;
-        }
+        cudaError_t e = allow_smem((const void*)pe_trace_kernel<true>, 0);
+        if (e != cudaSuccess) return e;
         pe_trace_kernel<true><<<(unsigned)n_tiles, kPeThreads, smem, stream>>>(p, geo);
     } else {
-        static bool attr_set = false;
-        if (!attr_set) {
-            cudaError_t e = cudaFuncSetAttribute(pe_trace_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            if (e != cudaSuccess) return e;
-            attr_set = true;
-        }
+        cudaError_t e = allow_smem((const void*)pe_trace_kernel<false>, 1);
+        if (e != cudaSuccess) return e;
         pe_trace_kernel<false><<<(unsigned)n_tiles, kPeThreads, smem, stream>>>(p, geo);
     }
     return cudaGetLastError();
+}
+
+cudaError_t pe_batch_launch(const PeBatchGeom* geoms, int n_geoms, long long total, unsigned long long* counter,
+                            int grid, cudaStream_t stream) {
+    if (total <= 0) return cudaSuccess;
+    if (n_geoms < 1 || n_geoms > kBatchConst) return cudaErrorInvalidValue;
+    cudaError_t e = allow_smem((const void*)pe_batch_kernel, 2);
+    if (e != cudaSuccess) return e;
+    e = cudaMemcpyToSymbolAsync(c_batch, geoms, sizeof(PeBatchGeom) * (size_t)n_geoms, 0, cudaMemcpyDeviceToDevice,
+                                stream);
+    if (e != cudaSuccess) return e;
+    e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), stream);
+    if (e != cudaSuccess) return e;
+    pe_batch_kernel<<<grid, kPeThreads, sizeof(PeSmem), stream>>>(n_geoms, total, counter);
+    return cudaGetLastError();
+}
+
+int pe_batch_blocks_per_sm() {
+    int n = 0;
+    if (allow_smem((const void*)pe_batch_kernel, 2) != cudaSuccess) return 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, pe_batch_kernel, kPeThreads, sizeof(PeSmem)) != cudaSuccess)
+        return 1;
+    return n > 0 ? n : 1;
 }
 
 }  // namespace smb

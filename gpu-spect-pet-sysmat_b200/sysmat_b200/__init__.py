@@ -42,11 +42,11 @@ class PeOptions(ctypes.Structure):
                 ("flags", ctypes.c_int)]
 
     @staticmethod
-    def make(sv=(1, 1, 1), sc=(8, 16, 8), tile_voxels=(0, 0, 0)) -> "PeOptions":
+    def make(sv=(1, 1, 1), sc=(8, 16, 8), tile_voxels=(0, 0, 0), autotune: bool = False) -> "PeOptions":
         o = PeOptions()
         for i in range(3):
             o.sv[i], o.sc[i], o.tile_voxels[i] = int(sv[i]), int(sc[i]), int(tile_voxels[i])
-        o.flags = 0
+        o.flags = 1 if autotune else 0
         return o
 
 
@@ -96,6 +96,13 @@ PROTOTYPES = {
     "sm_pe_set_counters": (ctypes.c_int, [_vp, ctypes.c_int]),
     "sm_pe_last_counters": (ctypes.c_int, [_vp, _i64p]),
     "sm_primitive_batch": (ctypes.c_int, [ctypes.c_int, _f32p, ctypes.c_int64, _f32p]),
+    "sm_pe_autotune": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(PeOptions), ctypes.c_int, ctypes.POINTER(PeOptions),
+                                      ctypes.POINTER(ctypes.c_double)]),
+    "sm_pe_batch_create": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(_vp), ctypes.POINTER(PeOptions),
+                                          ctypes.POINTER(ctypes.c_int), ctypes.POINTER(_vp), _i64p, ctypes.POINTER(_vp)]),
+    "sm_pe_batch_info": (ctypes.c_int, [_vp, _i64p]),
+    "sm_pe_batch_run": (ctypes.c_int, [_vp, _vp]),
+    "sm_pe_batch_destroy": (ctypes.c_int, [_vp]),
     "sm_scatter_options_reference": (None, [ctypes.POINTER(ScatterOptions)]),
     "sm_scatter_bitmap_words": (ctypes.c_int, [_vp, _i64p]),
     "sm_scatter_bitmaps": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_int, _vp]),
@@ -334,6 +341,54 @@ def pe_compute_static(p, dst_ptr: int, ld: int, rotation: int = 0, rows: Optiona
     _check(lib().sm_pe_compute_static(_fptr(col), col.size, _fptr(det), det.size, _fptr(img), img.size,
                                       ctypes.byref(opts), int(rotation), int(r0), int(r1), int(z0), int(nz),
                                       _vp(int(dst_ptr)), int(ld), _vp(stream)))
+
+
+def autotune(geo: "Geometry", opts: Optional[PeOptions] = None, rotation: int = 0):
+    """Brick (tile_voxels) the autotuner picks for ``geo``; returns
+    (options with that brick, ms per tile or -1 for a cached answer)."""
+    opts = opts if opts is not None else geo.options()
+    out = PeOptions()
+    ms = ctypes.c_double(0)
+    _check(lib().sm_pe_autotune(geo.ctx.handle, geo.handle, ctypes.byref(opts), int(rotation), ctypes.byref(out),
+                                ctypes.byref(ms)))
+    return out, ms.value
+
+
+class PeBatch:
+    """Whole PE sysmats of many geometries in one persistent launch (a CUDA
+    graph after the first run).  ``outputs``: device pointers, one [N][ld]
+    float32 buffer per geometry."""
+
+    def __init__(self, ctx: Context, geometries: Sequence["Geometry"], opts: Sequence[PeOptions],
+                 outputs: Sequence[int], lds: Sequence[int], rotations: Optional[Sequence[int]] = None):
+        n = len(geometries)
+        geos = (_vp * n)(*[g.handle for g in geometries])
+        op = (PeOptions * n)(*opts)
+        dst = (_vp * n)(*[_vp(int(o)) for o in outputs])
+        ld = np.ascontiguousarray(lds, dtype=np.int64)
+        rot = None if rotations is None else (ctypes.c_int * n)(*[int(r) for r in rotations])
+        h = _vp()
+        _check(lib().sm_pe_batch_create(ctx.handle, n, geos, op, rot, dst, ld.ctypes.data_as(_i64p), ctypes.byref(h)))
+        self.handle, self.ctx, self._keep = h, ctx, (geos, op, dst, ld, rot, list(geometries))
+
+    def info(self):
+        out = np.zeros(3, dtype=np.int64)
+        _check(lib().sm_pe_batch_info(self.handle, out.ctypes.data_as(_i64p)))
+        return {"geometries": int(out[0]), "items": int(out[1]), "ctas": int(out[2])}
+
+    def run(self, stream: int = 0):
+        _check(lib().sm_pe_batch_run(self.handle, _vp(stream)))
+
+    def close(self):
+        if self.handle:
+            lib().sm_pe_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def scatter_legacy(parts: str, collimator, detector, image, physics, pe: np.ndarray, geo_crystal: Optional[str],

@@ -96,9 +96,11 @@ int sm_geometry_info(const sm_geometry* geo, int64_t out[7]);
 typedef struct sm_pe_options {
     int sv[3];          /* voxel sub-samples (x, y, z); the entry is their mean  */
     int sc[3];          /* crystal sub-cells (x, y = depth, z); summed           */
-    int tile_voxels[3]; /* voxel brick per CTA; 0 = autotuned / default          */
-    int flags;          /* reserved, 0                                           */
+    int tile_voxels[3]; /* voxel brick per CTA; 0 = default (8 x 4 x 4)          */
+    int flags;          /* SM_PE_AUTOTUNE: choose tile_voxels with sm_pe_autotune */
 } sm_pe_options;
+
+enum { SM_PE_AUTOTUNE = 1 };
 
 /* Reference mode: sv = 1x1x1, sc = 8x16x8 (PESysMatGen.cu:435-440). */
 void sm_pe_options_reference(sm_pe_options* opt);
@@ -152,6 +154,34 @@ int sm_pe_record_hits(sm_context* ctx, const sm_geometry* geo, const sm_pe_optio
  * (costs a little time and synchronises the call). */
 int sm_pe_set_counters(sm_context* ctx, int enable);
 int sm_pe_last_counters(sm_context* ctx, int64_t out[4]);
+
+/* ---- batched photoelectric sysmats, brick autotuning ------------------------- */
+/* No reference counterpart (the reference runs one geometry per process).  A
+ * design sweep: many geometries of uneven size computed by one persistent
+ * kernel launch that hands out (geometry, tile) work items, largest first,
+ * replayed from a CUDA graph. */
+typedef struct sm_pe_batch sm_pe_batch;
+
+/* Times candidate voxel bricks on a sample of tiles of `geo` and writes the
+ * fastest into out->tile_voxels (out = *opt otherwise).  Results are cached
+ * per device and geometry class for the process, and appended to the file
+ * named by the environment variable SYSMAT_B200_TUNE_CACHE when it is set.
+ * best_ms_per_tile (may be NULL) receives the winner's time, -1 for a cache hit. */
+int sm_pe_autotune(sm_context* ctx, const sm_geometry* geo, const sm_pe_options* opt, int rotation,
+                   sm_pe_options* out, double* best_ms_per_tile);
+
+/* The whole PE sysmat of each of n geometries (all rows, all voxels, rotation
+ * rotations[i] or 0 when rotations is NULL) into device buffers dst[i] with
+ * row pitch ld[i].  Options with SM_PE_AUTOTUNE are autotuned here. */
+int sm_pe_batch_create(sm_context* ctx, int n, const sm_geometry* const* geos, const sm_pe_options* opts,
+                       const int* rotations, float* const* dst, const int64_t* ld, sm_pe_batch** out);
+/* out[0] geometries, out[1] work items, out[2] persistent CTAs */
+int sm_pe_batch_info(const sm_pe_batch* batch, int64_t out[3]);
+/* One launch of the batch on `stream` (asynchronous; sm_context_sync reports
+ * device-side capacity errors).  The first call captures the launch in a
+ * CUDA graph; later calls replay it. */
+int sm_pe_batch_run(sm_pe_batch* batch, void* stream);
+int sm_pe_batch_destroy(sm_pe_batch* batch);
 
 /* ---- primary-Compton scatter sysmat ------------------------------------------ */
 typedef struct sm_scatter_options {

@@ -1,0 +1,79 @@
+"""The batched photoelectric sysmat (one persistent launch over many
+geometries, replayed from a CUDA graph) and the brick autotuner.  Each
+geometry's matrix must equal, bit for bit, what sm_pe_compute gives for it
+alone: the decomposition into tiles never changes a value."""
+import numpy as np
+import pytest
+
+import sysmat_b200
+from sysmat_b200 import configs
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = sysmat_b200.Context(0)
+    yield c
+    c.close()
+
+
+def test_batch_equals_per_geometry_launches(ctx):
+    import torch
+    params = [configs.tiny(layers=3), configs.two_plates_small(seed=8), configs.tiny(seed=4, rotated=True),
+              configs.sweep()[2]]
+    geos = [sysmat_b200.Geometry(ctx, p) for p in params]
+    opts = [g.options() for g in geos]
+    opts[1] = geos[1].options(tile_voxels=(4, 4, 2))
+    rotations = [0, 0, 1, 0]
+    outs = [torch.full((g.n_crystals, g.nx * g.ny * g.nz), float("nan"), device="cuda") for g in geos]
+    batch = sysmat_b200.PeBatch(ctx, geos, opts, [o.data_ptr() for o in outs], [o.shape[1] for o in outs], rotations)
+    info = batch.info()
+    assert info["geometries"] == 4 and info["items"] > 0 and info["ctas"] >= 148
+    for rep in range(2):                      # first run captures the graph, the second replays it
+        for o in outs:
+            o.fill_(float("nan"))
+        batch.run()
+        torch.cuda.synchronize()
+        ctx.sync()
+        for g, o, op, rot in zip(geos, outs, opts, rotations):
+            ref = g.pe(rotation=rot, opts=op)
+            assert np.array_equal(o.cpu().numpy(), ref)
+    batch.close()
+    for g in geos:
+        g.close()
+
+
+def test_autotune_picks_a_brick_and_caches_it(ctx):
+    p = configs.two_plates_small(seed=8)
+    g = sysmat_b200.Geometry(ctx, p)
+    tuned, ms = sysmat_b200.autotune(g)
+    brick = tuple(tuned.tile_voxels)
+    assert all(b >= 1 for b in brick) and np.prod(brick) <= 128 and ms > 0
+    again, ms2 = sysmat_b200.autotune(g)
+    assert tuple(again.tile_voxels) == brick and ms2 == -1.0
+    # results do not depend on the brick
+    assert np.array_equal(g.pe(opts=tuned), g.pe())
+    auto = g.options()
+    auto.flags = 1
+    assert np.array_equal(g.pe(opts=auto), g.pe())
+    g.close()
+
+
+def test_batch_beyond_one_constant_table(ctx):
+    """More geometries than one persistent launch takes (64): the graph holds
+    one launch per chunk of 64."""
+    import torch
+    params = [configs.tiny(seed=s, layers=1 + s % 3) for s in range(67)]
+    geos = [sysmat_b200.Geometry(ctx, p) for p in params]
+    outs = [torch.full((g.n_crystals, g.nx * g.ny * g.nz), float("nan"), device="cuda") for g in geos]
+    batch = sysmat_b200.PeBatch(ctx, geos, [g.options() for g in geos], [o.data_ptr() for o in outs],
+                                [o.shape[1] for o in outs])
+    batch.run()
+    torch.cuda.synchronize()
+    ctx.sync()
+    for g, o in zip(geos, outs):
+        assert np.array_equal(o.cpu().numpy(), g.pe())
+    batch.close()
+    for g in geos:
+        g.close()
