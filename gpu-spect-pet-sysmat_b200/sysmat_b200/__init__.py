@@ -103,6 +103,9 @@ PROTOTYPES = {
     "sm_pe_batch_info": (ctypes.c_int, [_vp, _i64p]),
     "sm_pe_batch_run": (ctypes.c_int, [_vp, _vp]),
     "sm_pe_batch_destroy": (ctypes.c_int, [_vp]),
+    "sm_gemm_bf16": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, ctypes.c_int64, ctypes.c_int64, _vp,
+                                    ctypes.c_int64, ctypes.c_int64, _vp, ctypes.c_int64, ctypes.c_float, _vp, _vp,
+                                    ctypes.c_int, ctypes.c_int, _vp, _vp]),
     "sm_scatter_options_reference": (None, [ctypes.POINTER(ScatterOptions)]),
     "sm_scatter_bitmap_words": (ctypes.c_int, [_vp, _i64p]),
     "sm_scatter_bitmaps": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_int, _vp]),
@@ -389,6 +392,16 @@ class PeBatch:
             self.close()
         except Exception:
             pass
+
+
+def gemm_bf16(m: int, n: int, k: int, a: int, a_strides, b: int, b_strides, c: int, ldc: int, alpha: float = 1.0,
+              row_scale: int = 0, bias: int = 0, accumulate: bool = False, n_tile: int = 256, error: int = 0,
+              stream: int = 0):
+    """The surrogate's tcgen05 BF16 GEMM on device pointers (see sm_gemm_bf16)."""
+    _check(lib().sm_gemm_bf16(int(m), int(n), int(k), _vp(a), int(a_strides[0]), int(a_strides[1]), _vp(b),
+                              int(b_strides[0]), int(b_strides[1]), _vp(c), int(ldc), float(alpha),
+                              _vp(row_scale) if row_scale else None, _vp(bias) if bias else None, 1 if accumulate else 0,
+                              int(n_tile), _vp(error) if error else None, _vp(stream)))
 
 
 def scatter_legacy(parts: str, collimator, detector, image, physics, pe: np.ndarray, geo_crystal: Optional[str],

@@ -233,6 +233,19 @@ int sm_scatter_legacy(int parts, float* parameter_Collimator, float* parameter_D
                       float* parameter_Physics, float* PE_SysMat, const char* geo_crystal,
                       const char* geo_collimator, float* dst, int cuda_id);
 
+/* ---- scatter surrogate building blocks ----------------------------------------- */
+/* No reference counterpart.  BF16 tensor-core GEMM (tcgen05.mma, fp32
+ * accumulators in tensor memory) on device buffers of the current device:
+ *   C[i][j] = s_i * sum_k A[i][k] B[j][k] (+ bias[j]) (+ C[i][j] if accumulate)
+ * with A[i][k] = a[i * a_ms + k * a_ks], B[j][k] = b[j * b_ns + k * b_ks]
+ * (bf16, any strides; k-contiguous operands load fastest), C fp32 row-major
+ * with pitch ldc, s_i = row_scale[i] or alpha.  n_tile (64 / 128 / 256) is
+ * the column width per CTA.  error (device int, may be NULL) is set to 1 if
+ * the kernel's bounded wait on its own MMAs ran out.  Asynchronous on stream. */
+int sm_gemm_bf16(int m, int n, int k, const void* a, int64_t a_ms, int64_t a_ks, const void* b, int64_t b_ns,
+                 int64_t b_ks, float* c, int64_t ldc, float alpha, const float* row_scale, const float* bias,
+                 int accumulate, int n_tile, int* error, void* stream);
+
 /* Diagnostic: evaluate the tracer's ray primitives on the current device for
  * n argument rows (host arrays).  kind 0: chord through a box (12 floats:
  * segment in, out, box min, max), 1: chord from box entry to segment end
