@@ -35,4 +35,18 @@ inline int check_cuda(cudaError_t e, const char* what) {
 
 #define SM_CUDA(expr) SM_TRY(::smb::check_cuda((expr), #expr))
 
+// Stream-ordered device buffer, released on the same stream.
+struct DevBuf {
+    void* p = nullptr;
+    cudaStream_t s = nullptr;
+    int alloc(size_t bytes, cudaStream_t stream, const char* what) {
+        s = stream;
+        return check_cuda(cudaMallocAsync(&p, bytes ? bytes : 16, stream), what);
+    }
+    ~DevBuf() {
+        if (p) cudaFreeAsync(p, s);
+    }
+};
+
+
 }  // namespace smb

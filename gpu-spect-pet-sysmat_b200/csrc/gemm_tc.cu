@@ -25,14 +25,13 @@
 #include <cuda_runtime.h>
 
 #include "gemm_tc.h"
+#include "tc_common.cuh"
 
 namespace smb {
 namespace {
 
-constexpr int kTileM = 128;
-constexpr int kChunkK = 64;
+using namespace tc;
 constexpr int kGemmThreads = 128;
-constexpr uint32_t kWaitLimit = 1u << 26;   // mbarrier polls before giving up (seconds at worst)
 
 struct __align__(128) GemmSmem {
     __nv_bfloat16 a[kTileM * kChunkK];       // 16 KB
@@ -41,49 +40,6 @@ struct __align__(128) GemmSmem {
     uint32_t tmem_base;
     int failed;
 };
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-// Shared-memory matrix descriptor (tcgen05), no swizzle, K-major.
-__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo_bytes, uint32_t sbo_bytes) {
-    uint64_t d = 0;
-    d |= (uint64_t)((addr >> 4) & 0x3FFFu);              // start address, bits [0, 14)
-    d |= (uint64_t)((lbo_bytes >> 4) & 0x3FFFu) << 16;   // leading byte offset, bits [16, 30)
-    d |= (uint64_t)((sbo_bytes >> 4) & 0x3FFFu) << 32;   // stride byte offset, bits [32, 46)
-    d |= (uint64_t)1 << 46;                              // descriptor version (sm_100)
-    return d;                                            // base offset 0, layout type 0 = no swizzle
-}
-
-// Instruction descriptor: kind::f16, A = B = BF16, D = F32, both K-major, M = 128.
-__host__ __device__ constexpr uint32_t instr_desc(int n_tile) {
-    return (1u << 4)                                     // D format F32
-           | (1u << 7)                                   // A format BF16
-           | (1u << 10)                                  // B format BF16
-           | ((uint32_t)(n_tile >> 3) << 17)             // N / 8
-           | ((uint32_t)(kTileM >> 4) << 24);            // M / 16
-}
-
-__device__ __forceinline__ void mbar_init(unsigned long long* bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, uint32_t phase) {
-    const uint32_t a = smem_u32(bar);
-    for (uint32_t it = 0; it < kWaitLimit; ++it) {
-        uint32_t done;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-            "selp.b32 %0, 1, 0, p;\n\t}"
-            : "=r"(done)
-            : "r"(a), "r"(phase)
-            : "memory");
-        if (done) return true;
-    }
-    return false;
-}
 
 // Stages rows [r0, r0 + rows) x k [k0, k0 + 64) of a strided bf16 operand into
 // the core-matrix layout; rows beyond `rows_total` and k beyond `k_total` are zero.
@@ -105,8 +61,7 @@ __device__ __forceinline__ void stage(__nv_bfloat16* dst, int n_rows, const __nv
                 val = *reinterpret_cast<const uint4*>(t);
             }
         }
-        const int off = (((r >> 3) * 8 + kc) * 8 + (r & 7)) * 8;   // elements
-        *reinterpret_cast<uint4*>(dst + off) = val;
+        *reinterpret_cast<uint4*>(dst + core_offset(r, kc)) = val;
     }
 }
 
@@ -121,11 +76,7 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_bf16_tc_kernel(GemmArgs g) 
         S.failed = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    if (warp == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&S.tmem_base)),
-                     "r"((uint32_t)g.n_tile));
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
-    }
+    if (warp == 0) tmem_alloc(&S.tmem_base, (uint32_t)g.n_tile);
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;");
@@ -142,25 +93,7 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_bf16_tc_kernel(GemmArgs g) 
         // generic-proxy stores must be visible to the tensor core's async proxy
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
-        if (threadIdx.x == 0) {
-            asm volatile("tcgen05.fence::after_thread_sync;");
-            const uint32_t a_addr = smem_u32(S.a), b_addr = smem_u32(S.b);
-#pragma unroll
-            for (int j = 0; j < kChunkK / 16; ++j) {
-                const uint64_t da = smem_desc(a_addr + 256u * j, 128u, 1024u);
-                const uint64_t db = smem_desc(b_addr + 256u * j, 128u, 1024u);
-                const uint32_t accumulate = (c > 0 || j > 0) ? 1u : 0u;
-                asm volatile(
-                    "{\n\t.reg .pred p;\n\t"
-                    "setp.ne.b32 p, %4, 0;\n\t"
-                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
-                    :
-                    : "r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
-            }
-            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                             smem_u32(&S.mbar))
-                         : "memory");
-        }
+        if (threadIdx.x == 0) mma_chunk(tmem, S.a, S.b, idesc, c == 0, &S.mbar);
         // the MMAs must finish reading the buffers before they are refilled
         if (!mbar_wait(&S.mbar, phase)) {
             S.failed = 1;
@@ -178,25 +111,22 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_bf16_tc_kernel(GemmArgs g) 
         const int row = m0 + warp * 32 + lane;
         const float scale = (g.row_scale && row < g.m) ? g.row_scale[row] : g.alpha;
         for (int c0 = 0; c0 < g.n_tile; c0 += 16) {
-            uint32_t r[16];
-            const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
-            asm volatile(
-                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
-                "%14, %15}, [%16];"
-                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-                : "r"(taddr));
-            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            float r[16];
+            tmem_load16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, r);
             if (row < g.m) {
                 float* out = g.c + (long long)row * g.ldc + n0 + c0;
 #pragma unroll
                 for (int e = 0; e < 16; ++e) {
                     const int col = n0 + c0 + e;
                     if (col < g.n) {
-                        float v = __uint_as_float(r[e]) * scale;
-                        if (g.bias) v += g.bias[col];
-                        if (g.accumulate) v += out[e];
-                        out[e] = v;
+                        if (g.epilogue == 1) {
+                            out[e] = out[e] * __expf(r[e] * scale);
+                        } else {
+                            float v = r[e] * scale;
+                            if (g.bias) v += g.bias[col];
+                            if (g.accumulate) v += out[e];
+                            out[e] = v;
+                        }
                     }
                 }
             }
@@ -208,9 +138,7 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_bf16_tc_kernel(GemmArgs g) 
     }
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
-    if (warp == 0) {
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)g.n_tile));
-    }
+    if (warp == 0) tmem_dealloc(tmem, (uint32_t)g.n_tile);
 }
 
 }  // namespace

@@ -8,8 +8,9 @@
 
 namespace smb {
 
-// C[m][n] = s_m * sum_k A[m][k] B[n][k] (+ bias[n]) (+ C[m][n] if accumulate),
-// s_m = row_scale[m] when row_scale is set, else alpha.
+// epilogue 0: C[m][n] = s_m * acc (+ bias[n]) (+ C[m][n] if accumulate)
+// epilogue 1: C[m][n] = C[m][n] * exp(s_m * acc)            (multiplicative correction)
+// acc = sum_k A[m][k] B[n][k], s_m = row_scale[m] when row_scale is set, else alpha.
 struct GemmArgs {
     int m, n, k;
     const __nv_bfloat16* a;
@@ -22,6 +23,7 @@ struct GemmArgs {
     const float* row_scale;
     const float* bias;
     int accumulate;
+    int epilogue;
     int n_tile;                  // 64, 128 or 256 columns per CTA (TMEM columns)
     int* error;                  // set to 1 when a bounded wait runs out (may be null)
 };

@@ -20,6 +20,8 @@
 #include <cuda_runtime.h>
 
 #include "geometry.h"
+#include "common.h"
+#include "sysmat_b200.h"
 
 namespace smb {
 
@@ -72,6 +74,12 @@ struct ScatterParams {
     int dst_row0;
     // bricks
     int bricks_x, bricks_y, n_bricks;
+    // voxel subset: when cols is set, the voxels are the y-columns (x, z) = cols[i]
+    // (bricks of 8 columns x 32 y) and output column of (i, y) is i * ny + y
+    const int2* cols;
+    int n_cols;
+    const int* slot;             // when set: dst row of rank r is slot[r] (row-list mode)
+    const int* pair_col;         // when set: pair column of rank r is pair_col[r] (shared pair table)
     // inputs
     const float* pe;             // crystal kind: [N][ld_pe] photoelectric sysmat of the rotation
     long long ld_pe;
@@ -107,10 +115,51 @@ cudaError_t launch_bitmap_collimator(uint32_t* words, int64_t n_words, const Sca
 cudaError_t launch_scatter_pairs(int kind, const DevGeometry& G, const ScatterTables& T, const uint32_t* bitmap,
                                  const int* perm, int r0, int r1, float4* pair, cudaStream_t s);
 
-// Ranks of detectors [row0, row1) in spatial order (see ScatterParams::perm).
+// Ranks of detectors [row0, row1) (or of the listed ones) in spatial order (see ScatterParams::perm).
 std::vector<int> spatial_order(const HostGeometry& g, int row0, int row1);
+std::vector<int> spatial_order_of(const HostGeometry& g, const std::vector<int>& ids);
+
+// Which rows and voxels exact_scatter computes:
+//  * rows: [row0, row1) with dst row d - row0, or the listed (distinct)
+//    detectors with dst row i for detector (*rows)[i];
+//  * voxels: all (dst column = voxel index), or the y-columns (x, z) of the
+//    device list d_cols (dst column = i * ny + y).
+//  * rows_in_place: listed rows write dst row d itself instead of row i;
+//  * accumulate: add to dst instead of overwriting it.
+struct ExactSpec {
+    int row0 = 0, row1 = 0;
+    const std::vector<int>* rows = nullptr;
+    bool rows_in_place = false;
+    bool accumulate = false;
+    // crystal pair table computed beforehand (crystal_pair_table) for every
+    // detector, columns in spatial_order(0, N); null: computed here
+    const float4* pairs = nullptr;
+    const std::vector<int>* pairs_order = nullptr;
+    const int2* d_cols = nullptr;
+    int n_cols = 0;
+};
+
+int exact_scatter(const sm_geometry* geo, const int sp[3], int parts, float angle, const float* d_pe, int64_t ld_pe,
+                  const uint32_t* d_bm_crystal, const uint32_t* d_bm_collimator, const ExactSpec& spec, float* d_dst,
+                  int64_t ld, cudaStream_t s);
+// K[a][d][s] (row pitch ldk, anchor pitch N * ldk) = crystal-scatter entry of
+// detector d per unit PE of source s with the photon arriving from vbar[a][s]
+// (fractional voxel indices in x, y, z; w > 0 marks a source in use), a < n_anchors.
+// K is fp32, or bf16 when k_bf16.  With a shared pair table (pairs, its
+// device order d_order = spatial_order(0, N)) row r of K is detector d_order[r];
+// without one, row d is detector d.
+int scatter_transfer(const sm_geometry* geo, const int sp[3], float angle, const float4* d_vbar, int n_anchors, void* d_K,
+                     int64_t ldk, bool k_bf16, const float4* pairs, const int* d_order, cudaStream_t s);
+
+// The crystal pair table of every detector: [N * points][N] float4, column r
+// for detector (*order)[r], order = spatial_order(0, N) (also uploaded to d_order).
+int crystal_pair_table(const sm_geometry* geo, const int sp[3], DevBuf* table, std::vector<int>* order, DevBuf* d_order,
+                       cudaStream_t s);
 cudaError_t launch_brick_sources(const ScatterParams& P, const ScatterTables& T, uint32_t* brick_sources,
                                  cudaStream_t s);
+cudaError_t launch_scatter_transfer(const ScatterParams& P, const DevGeometry& G, const ScatterTables& T,
+                                    const float4* vbar, int n_anchors, void* K, bool k_bf16, long long ldk,
+                                    long long anchor_stride, cudaStream_t s);
 cudaError_t launch_scatter_main(const ScatterParams& P, const DevGeometry& G, const ScatterTables& T,
                                 cudaStream_t s);
 

@@ -18,19 +18,6 @@
 namespace smb {
 namespace {
 
-// Stream-ordered device buffer, released on the same stream.
-struct DevBuf {
-    void* p = nullptr;
-    cudaStream_t s = nullptr;
-    int alloc(size_t bytes, cudaStream_t stream, const char* what) {
-        s = stream;
-        return check_cuda(cudaMallocAsync(&p, bytes ? bytes : 16, stream), what);
-    }
-    ~DevBuf() {
-        if (p) cudaFreeAsync(p, s);
-    }
-};
-
 constexpr size_t kPairBudget = size_t(512) << 20;   // bytes of pair data per detector chunk
 
 int upload_tables(const HostScatterTables& H, int n_crystals, int n_holes0, cudaStream_t s, DevBuf* blob,
@@ -94,11 +81,14 @@ void fill_common(const HostGeometry& g, int rotation_index_unused, float angle, 
     P->n_bricks = P->bricks_x * P->bricks_y * g.nz;
 }
 
-// Both parts (mask bit 0 crystal, bit 1 collimator) into device dst rows [row0, row1).
-int scatter_device(sm_context* ctx, const sm_geometry* geo, const int sp[3], int parts, float angle, const float* d_pe,
-                   int64_t ld_pe, const uint32_t* d_bm_crystal, const uint32_t* d_bm_collimator, int row0, int row1,
-                   float* d_dst, int64_t ld, cudaStream_t s) {
-    (void)ctx;
+}  // namespace
+
+// Both parts (mask bit 0 crystal, bit 1 collimator) into device dst; rows and
+// voxels as `spec` says (see ExactSpec in scatter.h).
+int exact_scatter(const sm_geometry* geo, const int sp[3], int parts, float angle, const float* d_pe, int64_t ld_pe,
+                  const uint32_t* d_bm_crystal, const uint32_t* d_bm_collimator, const ExactSpec& spec, float* d_dst,
+                  int64_t ld, cudaStream_t s) {
+    const int row0 = spec.rows ? 0 : spec.row0, row1 = spec.rows ? (int)spec.rows->size() : spec.row1;
     const HostGeometry& g = geo->host;
     const int N = g.n_crystals;
     const int h0 = holes0_of(g);
@@ -110,23 +100,46 @@ int scatter_device(sm_context* ctx, const sm_geometry* geo, const int sp[3], int
 
     ScatterParams P{};
     fill_common(g, 0, angle, &P);
-    const std::vector<int> order = spatial_order(g, row0, row1);
+    const std::vector<int> order = spec.rows ? spatial_order_of(g, *spec.rows) : spatial_order(g, row0, row1);
+    // row-list mode: rank r writes the dst row of detector order[r] in the caller's list
+    std::vector<int> slot;
+    if (spec.rows) {
+        std::vector<int> where(N, -1);
+        for (size_t i = 0; i < spec.rows->size(); ++i) {
+            const int d = (*spec.rows)[i];
+            if (d < 0 || d >= N || where[d] >= 0) return fail(SM_ERR_INVALID, "row list: entry %zu (%d) is out of range or repeated", i, d);
+            where[d] = (int)i;
+        }
+        slot.resize(order.size());
+        for (size_t r = 0; r < order.size(); ++r) slot[r] = spec.rows_in_place ? order[r] : where[order[r]];
+    }
     DevBuf perm;
-    SM_TRY(perm.alloc(sizeof(int) * order.size(), s, "detector order"));
+    SM_TRY(perm.alloc(sizeof(int) * (order.size() + slot.size()), s, "detector order"));
     SM_CUDA(cudaMemcpyAsync(perm.p, order.data(), sizeof(int) * order.size(), cudaMemcpyHostToDevice, s));
-    SM_CUDA(cudaStreamSynchronize(s));   // the host order is released on return
+    if (!slot.empty())
+        SM_CUDA(cudaMemcpyAsync(static_cast<int*>(perm.p) + order.size(), slot.data(), sizeof(int) * slot.size(),
+                                cudaMemcpyHostToDevice, s));
+    SM_CUDA(cudaStreamSynchronize(s));   // the host vectors are released on return
     P.perm = static_cast<const int*>(perm.p);
+    P.slot = slot.empty() ? nullptr : static_cast<const int*>(perm.p) + order.size();
     P.dst_row0 = row0;
     P.dst = d_dst;
     P.ld = ld;
     P.pe = d_pe;
     P.ld_pe = ld_pe;
+    if (spec.d_cols) {
+        P.cols = spec.d_cols;
+        P.n_cols = spec.n_cols;
+        P.bricks_x = (spec.n_cols + kScBrickX - 1) / kScBrickX;
+        P.bricks_y = (g.ny + kScBrickY - 1) / kScBrickY;
+        P.n_bricks = P.bricks_x * P.bricks_y;
+    }
 
     DevBuf bm_c, bm_h, bricks, pairs;
     const uint32_t* bmc = d_bm_crystal;
     const uint32_t* bmh = d_bm_collimator;
     const bool do_crystal = (parts & 1) != 0, do_collimator = (parts & 2) != 0 && h0 > 0;
-    if (do_crystal && !bmc) {
+    if (do_crystal && !bmc && !spec.pairs) {
         const int64_t w = crystal_bitmap_words(N);
         SM_TRY(bm_c.alloc(sizeof(uint32_t) * (size_t)w, s, "crystal bitmap"));
         SM_CUDA(launch_bitmap_crystal(static_cast<uint32_t*>(bm_c.p), w, T, s));
@@ -149,9 +162,38 @@ int scatter_device(sm_context* ctx, const sm_geometry* geo, const int sp[3], int
     }
     const int kinds[2] = {kScatterCrystal, kScatterCollimator};
     const bool want[2] = {do_crystal, do_collimator};
+    DevBuf pcol;
     for (int ki = 0; ki < 2; ++ki) {
         if (!want[ki]) continue;
         const int kind = kinds[ki];
+        if (kind == kScatterCrystal && spec.pairs) {
+            // shared table: column of rank r is the rank of detector order[r] in the table's order
+            const std::vector<int>& all = *spec.pairs_order;
+            std::vector<int> where(N, -1), col(order.size());
+            for (int r = 0; r < (int)all.size(); ++r) where[all[r]] = r;
+            bool ident = true;
+            for (size_t r = 0; r < order.size(); ++r) {
+                col[r] = where[order[r]];
+                ident = ident && col[r] == (int)r;
+            }
+            ScatterParams Q = P;
+            Q.kind = kind;
+            Q.rank0 = 0;
+            Q.rank1 = row1 - row0;
+            Q.pair = spec.pairs;
+            Q.pair_r0 = 0;
+            Q.pair_ld = N;
+            if (!ident) {
+                SM_TRY(pcol.alloc(sizeof(int) * col.size(), s, "pair columns"));
+                SM_CUDA(cudaMemcpyAsync(pcol.p, col.data(), sizeof(int) * col.size(), cudaMemcpyHostToDevice, s));
+                SM_CUDA(cudaStreamSynchronize(s));
+                Q.pair_col = static_cast<const int*>(pcol.p);
+            }
+            Q.accumulate = (written || spec.accumulate) ? 1 : 0;
+            SM_CUDA(launch_scatter_main(Q, geo->dev.view, T, s));
+            written = true;
+            continue;
+        }
         const int n_src = kind == kScatterCrystal ? N * T.n_points : h0;
         int chunk = (int)std::max<size_t>(kScTileD, kPairBudget / (sizeof(float4) * (size_t)std::max(1, n_src)));
         chunk = std::max(kScTileD, chunk / kScTileD * kScTileD);
@@ -170,17 +212,103 @@ int scatter_device(sm_context* ctx, const sm_geometry* geo, const int sp[3], int
             Q.pair = static_cast<const float4*>(pair.p);
             Q.pair_r0 = c0;
             Q.pair_ld = c1 - c0;
-            Q.accumulate = written ? 1 : 0;
+            Q.accumulate = (written || spec.accumulate) ? 1 : 0;
             SM_CUDA(launch_scatter_main(Q, geo->dev.view, T, s));
         }
         written = true;
     }
-    if (!written) {
-        const int64_t vox = (int64_t)g.nx * g.ny * g.nz;
-        SM_CUDA(cudaMemset2DAsync(d_dst, sizeof(float) * (size_t)ld, 0, sizeof(float) * (size_t)vox, (size_t)(row1 - row0), s));
+    if (!written && !spec.accumulate) {
+        const int64_t vox = spec.d_cols ? (int64_t)spec.n_cols * g.ny : (int64_t)g.nx * g.ny * g.nz;
+        if (spec.rows && spec.rows_in_place) {
+            for (int d : *spec.rows) SM_CUDA(cudaMemsetAsync(d_dst + (int64_t)d * ld, 0, sizeof(float) * (size_t)vox, s));
+        } else {
+            SM_CUDA(cudaMemset2DAsync(d_dst, sizeof(float) * (size_t)ld, 0, sizeof(float) * (size_t)vox,
+                                      (size_t)(row1 - row0), s));
+        }
     }
     return SM_OK;
 }
+
+int crystal_pair_table(const sm_geometry* geo, const int sp[3], DevBuf* table, std::vector<int>* order, DevBuf* d_order,
+                       cudaStream_t s) {
+    const HostGeometry& g = geo->host;
+    const int N = g.n_crystals;
+    HostScatterTables H;
+    SM_TRY(build_scatter_tables(g, sp, &H));
+    DevBuf tables;
+    ScatterTables T;
+    SM_TRY(upload_tables(H, N, holes0_of(g), s, &tables, &T));
+    *order = spatial_order(g, 0, N);
+    SM_TRY(d_order->alloc(sizeof(int) * (size_t)N, s, "detector order"));
+    SM_CUDA(cudaMemcpyAsync(d_order->p, order->data(), sizeof(int) * (size_t)N, cudaMemcpyHostToDevice, s));
+    DevBuf bm;
+    const int64_t w = crystal_bitmap_words(N);
+    SM_TRY(bm.alloc(sizeof(uint32_t) * (size_t)w, s, "crystal bitmap"));
+    SM_CUDA(launch_bitmap_crystal(static_cast<uint32_t*>(bm.p), w, T, s));
+    const size_t n_src = (size_t)N * T.n_points;
+    SM_TRY(table->alloc(sizeof(float4) * n_src * (size_t)N, s, "crystal pair table"));
+    SM_CUDA(launch_scatter_pairs(kScatterCrystal, geo->dev.view, T, static_cast<const uint32_t*>(bm.p),
+                                 static_cast<const int*>(d_order->p), 0, N, static_cast<float4*>(table->p), s));
+    SM_CUDA(cudaStreamSynchronize(s));   // the host tables are released on return
+    return SM_OK;
+}
+
+int scatter_transfer(const sm_geometry* geo, const int sp[3], float angle, const float4* d_vbar, int n_anchors, void* d_K,
+                     int64_t ldk, bool k_bf16, const float4* pairs, const int* d_order, cudaStream_t s) {
+    const HostGeometry& g = geo->host;
+    const int N = g.n_crystals;
+    HostScatterTables H;
+    SM_TRY(build_scatter_tables(g, sp, &H));
+    DevBuf tables;
+    ScatterTables T;
+    SM_TRY(upload_tables(H, N, holes0_of(g), s, &tables, &T));
+    ScatterParams P{};
+    fill_common(g, 0, angle, &P);
+    P.kind = kScatterCrystal;
+    if (pairs) {
+        P.perm = d_order;
+        P.rank0 = 0;
+        P.rank1 = N;
+        P.pair = pairs;
+        P.pair_r0 = 0;
+        P.pair_ld = N;
+        SM_CUDA(launch_scatter_transfer(P, geo->dev.view, T, d_vbar, n_anchors, d_K, k_bf16, ldk, (long long)N * ldk, s));
+        SM_CUDA(cudaStreamSynchronize(s));
+        return SM_OK;
+    }
+    std::vector<int> ident(N);
+    for (int i = 0; i < N; ++i) ident[i] = i;
+    DevBuf perm, bm;
+    SM_TRY(perm.alloc(sizeof(int) * (size_t)N, s, "detector order"));
+    SM_CUDA(cudaMemcpyAsync(perm.p, ident.data(), sizeof(int) * (size_t)N, cudaMemcpyHostToDevice, s));
+    SM_CUDA(cudaStreamSynchronize(s));
+    P.perm = static_cast<const int*>(perm.p);
+    const int64_t w = crystal_bitmap_words(N);
+    SM_TRY(bm.alloc(sizeof(uint32_t) * (size_t)w, s, "crystal bitmap"));
+    SM_CUDA(launch_bitmap_crystal(static_cast<uint32_t*>(bm.p), w, T, s));
+    const int n_src = N * T.n_points;
+    int chunk = (int)std::max<size_t>(128, kPairBudget / (sizeof(float4) * (size_t)std::max(1, n_src)));
+    chunk = std::max(128, chunk / 128 * 128);
+    DevBuf pair;
+    SM_TRY(pair.alloc(sizeof(float4) * (size_t)n_src * (size_t)std::min(chunk, N), s, "scatter pairs"));
+    for (int c0 = 0; c0 < N; c0 += chunk) {
+        const int c1 = std::min(N, c0 + chunk);
+        SM_CUDA(launch_scatter_pairs(kScatterCrystal, geo->dev.view, T, static_cast<const uint32_t*>(bm.p), P.perm, c0, c1,
+                                     static_cast<float4*>(pair.p), s));
+        ScatterParams Q = P;
+        Q.rank0 = c0;
+        Q.rank1 = c1;
+        Q.pair = static_cast<const float4*>(pair.p);
+        Q.pair_r0 = c0;
+        Q.pair_ld = c1 - c0;
+        void* kc = static_cast<char*>(d_K) + (size_t)c0 * (size_t)ldk * (k_bf16 ? 2 : 4);
+        SM_CUDA(launch_scatter_transfer(Q, geo->dev.view, T, d_vbar, n_anchors, kc, k_bf16, ldk, (long long)N * ldk, s));
+    }
+    SM_CUDA(cudaStreamSynchronize(s));
+    return SM_OK;
+}
+
+namespace {
 
 int read_words(const char* path, std::vector<uint32_t>* out, int64_t n) {
     FILE* f = std::fopen(path, "rb");
@@ -220,6 +348,48 @@ int validate_scatter(const sm_geometry* geo, const sm_scatter_options* opt, int 
 using namespace smb;
 
 extern "C" {
+
+int sm_scatter_subset(sm_context* ctx, const sm_geometry* geo, const sm_scatter_options* opt, int rotation,
+                      const float* pe, int64_t ld_pe, const int32_t* rows, int n_rows, const int32_t* cols, int n_cols,
+                      float* dst, int64_t ld, void* stream_ptr) {
+    if (!geo || !opt || !dst || !rows || n_rows <= 0) return fail(SM_ERR_INVALID, "null argument or empty row list");
+    SM_TRY(context_bind(ctx));
+    SM_TRY(validate_scatter(geo, opt, 0, geo->host.n_crystals));
+    const HostGeometry& g = geo->host;
+    const int64_t V = (int64_t)g.nx * g.ny * g.nz;
+    if ((opt->parts & 1) && (!pe || ld_pe < V)) return fail(SM_ERR_INVALID, "crystal scatter needs the PE sysmat with ld_pe >= %lld", (long long)V);
+    const int64_t width = cols ? (int64_t)n_cols * g.ny : V;
+    if (cols && n_cols <= 0) return fail(SM_ERR_INVALID, "empty column list");
+    if (ld < width) return fail(SM_ERR_INVALID, "ld = %lld is smaller than the %lld output columns", (long long)ld, (long long)width);
+    cudaStream_t s = (cudaStream_t)stream_ptr;
+    std::vector<int> list(rows, rows + n_rows);
+    ExactSpec spec;
+    spec.rows = &list;
+    DevBuf cb;
+    if (cols) {
+        for (int c = 0; c < n_cols; ++c)
+            if (cols[2 * c] < 0 || cols[2 * c] >= g.nx || cols[2 * c + 1] < 0 || cols[2 * c + 1] >= g.nz)
+                return fail(SM_ERR_INVALID, "column %d (%d, %d) is outside the %d x %d grid", c, cols[2 * c], cols[2 * c + 1], g.nx, g.nz);
+        SM_TRY(cb.alloc(sizeof(int2) * (size_t)n_cols, s, "column list"));
+        SM_CUDA(cudaMemcpyAsync(cb.p, cols, sizeof(int2) * (size_t)n_cols, cudaMemcpyHostToDevice, s));
+        spec.d_cols = static_cast<const int2*>(cb.p);
+        spec.n_cols = n_cols;
+    }
+    const float angle = (float)rotation * g.angle_per_rotation;
+    return exact_scatter(geo, opt->sp, opt->parts, angle, (opt->parts & 1) ? pe : nullptr, ld_pe, nullptr, nullptr, spec,
+                         dst, ld, s);
+}
+
+int sm_scatter_transfer(sm_context* ctx, const sm_geometry* geo, const sm_scatter_options* opt, int rotation,
+                        const float* vbar, int n_anchors, float* K, int64_t ldk, void* stream) {
+    if (!geo || !opt || !vbar || !K || n_anchors <= 0) return fail(SM_ERR_INVALID, "null argument or no anchors");
+    SM_TRY(context_bind(ctx));
+    SM_TRY(validate_scatter(geo, opt, 0, geo->host.n_crystals));
+    if (ldk < geo->host.n_crystals) return fail(SM_ERR_INVALID, "ldk = %lld is smaller than N = %d", (long long)ldk, geo->host.n_crystals);
+    const float angle = (float)rotation * geo->host.angle_per_rotation;
+    return scatter_transfer(geo, opt->sp, angle, reinterpret_cast<const float4*>(vbar), n_anchors, K, ldk, false, nullptr,
+                            nullptr, (cudaStream_t)stream);
+}
 
 void sm_scatter_options_reference(sm_scatter_options* opt) {
     if (!opt) return;
@@ -331,7 +501,10 @@ int sm_scatter_compute(sm_context* ctx, const sm_geometry* geo, const sm_scatter
         SM_TRY(out_buf.alloc(sizeof(float) * (size_t)rows * (size_t)ld, s, "scatter output"));
         d_dst = static_cast<float*>(out_buf.p);
     }
-    SM_TRY(scatter_device(ctx, geo, opt->sp, opt->parts, angle, d_pe, ld_pe, d_bmc, d_bmh, row0, row1, d_dst, ld, s));
+    ExactSpec spec;
+    spec.row0 = row0;
+    spec.row1 = row1;
+    SM_TRY(exact_scatter(geo, opt->sp, opt->parts, angle, d_pe, ld_pe, d_bmc, d_bmh, spec, d_dst, ld, s));
     if (!dst_on_device) {
         SM_CUDA(cudaMemcpyAsync(dst, d_dst, sizeof(float) * (size_t)rows * (size_t)ld, cudaMemcpyDeviceToHost, s));
     }
@@ -418,7 +591,10 @@ int sm_scatter_legacy(int parts, float* parameter_Collimator, float* parameter_D
         }
         SM_TRY(out_buf.alloc(sizeof(float) * (size_t)N * (size_t)V, s, "scatter output"));
         float* d_out = static_cast<float*>(out_buf.p);
-        SM_TRY(scatter_device(ctx, geo, opt.sp, parts, angle, d_pe, V, d_bmc, d_bmh, 0, N, d_out, V, s));
+        ExactSpec spec;
+        spec.row0 = 0;
+        spec.row1 = N;
+        SM_TRY(exact_scatter(geo, opt.sp, parts, angle, d_pe, V, d_bmc, d_bmh, spec, d_out, V, s));
         SM_CUDA(cudaMemcpyAsync(out.data(), d_out, sizeof(float) * out.size(), cudaMemcpyDeviceToHost, s));
         SM_CUDA(cudaStreamSynchronize(s));
     }

@@ -194,12 +194,17 @@ int build_scatter_tables(const HostGeometry& g, const int sp[3], HostScatterTabl
 // one layer.  Lanes of a warp are detectors; a patch makes the energy-window
 // cull and the scattered photon's path coherent across the warp.
 std::vector<int> spatial_order(const HostGeometry& g, int row0, int row1) {
-    const int n = row1 - row0;
-    std::vector<int> ids(n);
-    for (int i = 0; i < n; ++i) ids[i] = row0 + i;
+    std::vector<int> ids(row1 - row0);
+    for (int i = 0; i < row1 - row0; ++i) ids[i] = row0 + i;
+    return spatial_order_of(g, ids);
+}
+
+std::vector<int> spatial_order_of(const HostGeometry& g, const std::vector<int>& ids_in) {
+    std::vector<int> ids = ids_in;
+    const int n = (int)ids.size();
     if (n <= 1) return ids;
     float tmin = 1e30f, wmin = 1e30f, xmin = 1e30f, zmin = 1e30f;
-    for (int d = row0; d < row1; ++d) {
+    for (int d : ids) {
         const float* sz = &g.c_size[4 * (size_t)d];
         const float* ps = &g.c_pos[4 * (size_t)d];
         tmin = std::min(tmin, sz[1]);
@@ -227,7 +232,7 @@ std::vector<int> spatial_order(const HostGeometry& g, int row0, int row1) {
         return x;
     };
     std::vector<uint64_t> key(g.n_crystals, 0);
-    for (int d = row0; d < row1; ++d) {
+    for (int d : ids) {
         const float* ps = &g.c_pos[4 * (size_t)d];
         const uint32_t ix = (uint32_t)std::min(65535.0f, std::max(0.0f, std::floor((ps[0] - xmin) / wmin + 0.5f)));
         const uint32_t iz = (uint32_t)std::min(65535.0f, std::max(0.0f, std::floor((ps[2] - zmin) / wmin + 0.5f)));

@@ -20,6 +20,7 @@
 // correction terms, whose remainder is below 1e-10.
 #include <algorithm>
 
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include "scatter.h"
@@ -210,23 +211,140 @@ __global__ void scatter_pair_kernel(DevGeometry G, ScatterTables T, const uint32
     }
 }
 
+// Column xx (0..7) of brick b: its (x, z), first y and whether it exists.
+struct BrickCol {
+    int x, z, y0, ci;            // ci: index in the column list (column mode)
+    bool valid;
+};
+
+__device__ __forceinline__ BrickCol brick_column(const ScatterParams& P, int b, int xx) {
+    BrickCol c;
+    if (P.cols) {
+        const int cg = b % P.bricks_x, by = b / P.bricks_x;
+        c.ci = cg * kScBrickX + xx;
+        c.valid = c.ci < P.n_cols;
+        const int2 xz = c.valid ? P.cols[c.ci] : make_int2(0, 0);
+        c.x = xz.x;
+        c.z = xz.y;
+        c.y0 = by * kScBrickY;
+    } else {
+        const int bx = b % P.bricks_x, by = (b / P.bricks_x) % P.bricks_y, bz = b / (P.bricks_x * P.bricks_y);
+        c.x = bx * kScBrickX + xx;
+        c.z = bz;
+        c.y0 = by * kScBrickY;
+        c.ci = 0;
+        c.valid = c.x < P.nx;
+    }
+    return c;
+}
+
 // ---- sources with PE != 0 per voxel brick -----------------------------------------
 __global__ void brick_sources_kernel(ScatterParams P, int N, uint32_t* __restrict__ out) {
     const int b = blockIdx.x;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int s = blockIdx.y * kScWarps + warp;
     if (s >= N) return;
-    const int bx = b % P.bricks_x, by = (b / P.bricks_x) % P.bricks_y, bz = b / (P.bricks_x * P.bricks_y);
-    const int x = bx * kScBrickX + (lane & 7);
+    const BrickCol bc = brick_column(P, b, lane & 7);
     bool any = false;
     for (int it = 0; it < kScBrickY / 4; ++it) {
-        const int y = by * kScBrickY + it * 4 + (lane >> 3);
-        if (x < P.nx && y < P.ny) {
-            const long long v = (long long)x + (long long)P.nx * (y + (long long)P.ny * bz);
+        const int y = bc.y0 + it * 4 + (lane >> 3);
+        if (bc.valid && y < P.ny) {
+            const long long v = (long long)bc.x + (long long)P.nx * (y + (long long)P.ny * bc.z);
             any |= __ldg(P.pe + (long long)s * P.ld_pe + v) != 0.0f;
         }
     }
     if (__any_sync(0xffffffffu, any) && lane == 0) atomicOr(out + (long long)b * P.src_words + (s >> 5), 1u << (s & 31));
+}
+
+// Detecting crystal d: geometry, energy window, switch (scatter.cu:1189-1205);
+// returns the per-detector factor of the kind (mu_c / mu_pe / points, or plate mu_c / mu_t).
+template <int KIND>
+__device__ __forceinline__ float setup_det(const ScatterParams& P, const DevGeometry& G, const ScatterTables& T, int d,
+                                           Det& D) {
+    const float4 pos = G.c.pos[d], sz = G.c.size[d], rt = G.c.rot[d], ph = G.c.phys[d];
+    D.x = pos.x; D.y = pos.y; D.z = pos.z; D.cm = rt.x; D.sm = rt.y;
+    D.hw = 0.5f * sz.x; D.ht = 0.5f * sz.y; D.hh = 0.5f * sz.z;
+    D.r_unit = sqrtf(sz.x * sz.x / 1.0f / 1.0f + sz.z * sz.z / 1.0f / 1.0f + sz.y * sz.y / 1.0f / 1.0f) / 2.0f;
+    D.mu_pe = ph.x; D.mu_c = ph.y; D.res = ph.z;
+    if (P.same_window > 0) { D.lo = P.win_lo; D.hi = P.win_hi; }
+    else {
+        D.lo = (1.0f - D.res / 2.0f) * P.e0;
+        D.hi = (1.0f + D.res / 2.0f) * P.e0;
+    }
+    D.on = P.use_compton == 1 && pos.w > 0.01f;   // (scatter.cu:1203-1205)
+    D.c_cut = window_cos_cut(P.e0, P.alpha, D.res, D.lo);
+    return KIND == kScatterCrystal ? D.mu_c / D.mu_pe / (float)T.n_points : P.plate_c_over_t;
+}
+
+// Voxel centre (world) of fractional voxel indices: FOV shift and image rotation (scatter.cu:1172-1184).
+__device__ __forceinline__ float3 voxel_world(const ScatterParams& P, float x, float y, float z) {
+    float xi = (x - (float)P.nx / 2.0f + 0.5f) * P.vx;
+    float yi = (y - (float)P.ny / 2.0f + 0.5f) * P.vy;
+    float zi = (z - (float)P.nz / 2.0f + 0.5f) * P.vz;
+    xi = xi + P.shx;
+    yi = yi + P.shy;
+    zi = zi + P.shz;
+    return make_float3(xi * P.cos_a - yi * P.sin_a, xi * P.sin_a + yi * P.cos_a, zi);
+}
+
+// ---- transfer of arrival points per source ------------------------------------------
+// K[a][r][s] = scale_d * sum_p term(vbar[a][s], s_p, d) for d = perm[r] and anchor a:
+// the crystal-scatter sysmat entry per unit PE of source s with every photon
+// arriving from vbar[a][s] (fractional voxel indices; w <= 0: source unused).
+// Thread = rank (coalesced pair reads), grid.y = source; the source point and
+// its pair sums are set up once for all anchors.
+constexpr int kMaxAnchorsPerPass = 8;
+
+template <typename KT>
+__global__ void scatter_transfer_kernel(ScatterParams P, DevGeometry G, ScatterTables T, const float4* __restrict__ vbar,
+                                        int n_anchors, KT* __restrict__ K, long long ldk, long long anchor_stride) {
+    __shared__ KnNode kn[kKnNodes + 1];
+    for (int i = threadIdx.x; i < kKnNodes + 1; i += blockDim.x) kn[i] = T.kn[i];
+    __syncthreads();
+    const int rank = P.rank0 + blockIdx.x * blockDim.x + threadIdx.x;
+    if (rank >= P.rank1) return;
+    const int d = P.perm[rank];
+    Det D;
+    const float scale = setup_det<kScatterCrystal>(P, G, T, d, D);
+    for (int s = blockIdx.y; s < T.n_crystals; s += gridDim.y) {
+        for (int a0 = 0; a0 < n_anchors; a0 += kMaxAnchorsPerPass) {
+            const int na = min(kMaxAnchorsPerPass, n_anchors - a0);
+            float acc[kMaxAnchorsPerPass];
+            float3 I[kMaxAnchorsPerPass], Is[kMaxAnchorsPerPass];
+            bool use[kMaxAnchorsPerPass];
+#pragma unroll
+            for (int j = 0; j < kMaxAnchorsPerPass; ++j) {
+                acc[j] = 0.0f;
+                use[j] = false;
+                if (j < na) {
+                    const float4 vb = vbar[(long long)(a0 + j) * T.n_crystals + s];
+                    use[j] = D.on && s != d && vb.w > 0.0f;
+                    I[j] = voxel_world(P, vb.x, vb.y, vb.z);
+                    Is[j] = make_float3((I[j].x - D.x) * D.cm - (I[j].z - D.z) * D.sm, I[j].y - D.y,
+                                        (I[j].x - D.x) * D.sm + (I[j].z - D.z) * D.cm);
+                }
+            }
+            bool any = false;
+#pragma unroll
+            for (int j = 0; j < kMaxAnchorsPerPass; ++j) any |= use[j];
+            if (any) {
+                for (int p = 0; p < T.n_points; ++p) {
+                    const int q = s * T.n_points + p;
+                    Src C;
+                    make_src_basic(D, T.crystal_src[q], C);
+                    make_src_rest(D, P.pair[(long long)q * P.pair_ld + (P.pair_col ? P.pair_col[rank] : rank - P.pair_r0)], C);
+#pragma unroll
+                    for (int j = 0; j < kMaxAnchorsPerPass; ++j)
+                        if (use[j])
+                            acc[j] += scatter_term(P, D, C, kn, T.kn_inv_norm, I[j].x, I[j].y, I[j].z, Is[j].x, Is[j].y,
+                                                   Is[j].z);
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < kMaxAnchorsPerPass; ++j)
+                if (j < na) K[(long long)(a0 + j) * anchor_stride + (long long)(rank - P.rank0) * ldk + s] = (KT)(acc[j] * scale);
+        }
+    }
 }
 
 struct __align__(16) ScSmem {
@@ -244,24 +362,19 @@ __global__ void __launch_bounds__(kScThreads, 2) scatter_main_kernel(ScatterPara
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int b = blockIdx.x % P.n_bricks;
     const int dt = blockIdx.x / P.n_bricks;
-    const int bx = b % P.bricks_x, by = (b / P.bricks_x) % P.bricks_y, bz = b / (P.bricks_x * P.bricks_y);
-    const int x0 = bx * kScBrickX, y0 = by * kScBrickY;
+    const BrickCol mycol = brick_column(P, b, warp);        // this warp's voxel column
+    const BrickCol stcol = brick_column(P, b, tid & 7);     // the column this thread stages
+    const int y0 = mycol.y0;
 
     for (int i = tid; i < kKnNodes + 1; i += kScThreads) S.kn[i] = T.kn[i];
     for (int i = tid; i < kScBrickX * kScBrickY * kScTileD; i += kScThreads) (&S.acc[0][0][0])[i] = 0.0;
     {
         const int xx = tid & 7, yy = tid >> 3;
-        const int x = x0 + xx, y = y0 + yy;
+        const int x = stcol.x, y = y0 + yy;
         float4 v = make_float4(0.0f, 0.0f, 0.0f, -1.0f);
-        if (x < P.nx && y < P.ny) {
-            // voxel centre, FOV shift, image rotation (scatter.cu:1172-1184)
-            float xi = ((float)x - (float)P.nx / 2.0f + 0.5f) * P.vx;
-            float yi = ((float)y - (float)P.ny / 2.0f + 0.5f) * P.vy;
-            float zi = ((float)bz - (float)P.nz / 2.0f + 0.5f) * P.vz;
-            xi = xi + P.shx;
-            yi = yi + P.shy;
-            zi = zi + P.shz;
-            v = make_float4(xi * P.cos_a - yi * P.sin_a, xi * P.sin_a + yi * P.cos_a, zi, 1.0f);
+        if (stcol.valid && y < P.ny) {
+            const float3 w = voxel_world(P, (float)x, (float)y, (float)stcol.z);
+            v = make_float4(w.x, w.y, w.z, 1.0f);
         }
         S.vox[xx][yy] = v;
     }
@@ -269,27 +382,12 @@ __global__ void __launch_bounds__(kScThreads, 2) scatter_main_kernel(ScatterPara
     const int rank = P.rank0 + dt * kScTileD + lane;
     const int d = rank < P.rank1 ? P.perm[rank] : -1;
     Det D;
-    D.on = rank < P.rank1;
+    D.on = false;
     float scale = 0.0f;
-    if (D.on) {
-        const float4 pos = G.c.pos[d], sz = G.c.size[d], rt = G.c.rot[d], ph = G.c.phys[d];
-        D.x = pos.x; D.y = pos.y; D.z = pos.z; D.cm = rt.x; D.sm = rt.y;
-        D.hw = 0.5f * sz.x; D.ht = 0.5f * sz.y; D.hh = 0.5f * sz.z;
-        D.r_unit = sqrtf(sz.x * sz.x / 1.0f / 1.0f + sz.z * sz.z / 1.0f / 1.0f + sz.y * sz.y / 1.0f / 1.0f) / 2.0f;
-        D.mu_pe = ph.x; D.mu_c = ph.y; D.res = ph.z;
-        if (P.same_window > 0) { D.lo = P.win_lo; D.hi = P.win_hi; }
-        else {
-            D.lo = (1.0f - D.res / 2.0f) * P.e0;
-            D.hi = (1.0f + D.res / 2.0f) * P.e0;
-        }
-        D.on = P.use_compton == 1 && pos.w > 0.01f;   // (scatter.cu:1203-1205)
-        D.c_cut = window_cos_cut(P.e0, P.alpha, D.res, D.lo);
-        scale = KIND == kScatterCrystal ? D.mu_c / D.mu_pe / (float)T.n_points : P.plate_c_over_t;
-    }
+    if (rank < P.rank1) scale = setup_det<KIND>(P, G, T, d, D);
     if (warp == 0) S.scale[lane] = scale;
     __syncthreads();
 
-    const int x = x0 + warp;
     const float inv_norm = T.kn_inv_norm;
     // this warp's voxel column: I0 + t e, t in [0, col_t] (image y axis, rotated)
     const float4 col0 = S.vox[warp][0];
@@ -306,8 +404,9 @@ __global__ void __launch_bounds__(kScThreads, 2) scatter_main_kernel(ScatterPara
                 {
                     const int xx = tid & 7, yy = tid >> 3;
                     float v = 0.0f;
-                    if (x0 + xx < P.nx && y0 + yy < P.ny)
-                        v = __ldg(P.pe + (long long)s * P.ld_pe + (x0 + xx) + (long long)P.nx * ((y0 + yy) + (long long)P.ny * bz));
+                    if (stcol.valid && y0 + yy < P.ny)
+                        v = __ldg(P.pe + (long long)s * P.ld_pe + stcol.x +
+                                  (long long)P.nx * ((y0 + yy) + (long long)P.ny * stcol.z));
                     S.pe[yy][xx] = v;
                 }
                 __syncthreads();
@@ -325,7 +424,10 @@ __global__ void __launch_bounds__(kScThreads, 2) scatter_main_kernel(ScatterPara
                         on = column_max_cos(C, col0.x, col0.y, col0.z, col_ex, col_ey, 0.0f, col_t) > D.c_cut;
                     }
                     if (!__any_sync(0xffffffffu, on)) continue;
-                    if (on) make_src_rest(D, P.pair[(long long)q * P.pair_ld + (rank - P.pair_r0)], C);
+                    if (on) {
+                        const long long pc = P.pair_col ? P.pair_col[rank] : rank - P.pair_r0;
+                        make_src_rest(D, P.pair[(long long)q * P.pair_ld + pc], C);
+                    }
                     unsigned m = live;
                     while (m) {
                         const int j = __ffs(m) - 1;
@@ -346,7 +448,7 @@ __global__ void __launch_bounds__(kScThreads, 2) scatter_main_kernel(ScatterPara
         for (int h = 0; h < T.n_holes0; ++h) {
             const float4 src = T.hole_src[h];
             Src C;
-            bool on = D.on && x < P.nx;
+            bool on = D.on && mycol.valid;
             if (on) {
                 make_src_basic(D, src, C);
                 on = column_max_cos(C, col0.x, col0.y, col0.z, col_ex, col_ey, 0.0f, col_t) > D.c_cut;
@@ -377,12 +479,16 @@ __global__ void __launch_bounds__(kScThreads, 2) scatter_main_kernel(ScatterPara
     const int n_rows = min(kScTileD, P.rank1 - (P.rank0 + dt * kScTileD));
     for (int i = tid; i < n_rows * kScBrickY * kScBrickX; i += kScThreads) {
         const int xx = i & 7, yy = (i >> 3) & 31, dl = i >> 8;
-        const int xv = x0 + xx, yv = y0 + yy;
-        if (xv >= P.nx || yv >= P.ny) continue;
-        const int dd = P.perm[P.rank0 + dt * kScTileD + dl];
+        const BrickCol oc = brick_column(P, b, xx);
+        const int yv = y0 + yy;
+        if (!oc.valid || yv >= P.ny) continue;
+        const int rk = P.rank0 + dt * kScTileD + dl;
+        const int dd = P.perm[rk];
         const float sc = S.scale[dl];
-        const long long col = (long long)xv + (long long)P.nx * (yv + (long long)P.ny * bz);
-        float* out = P.dst + (long long)(dd - P.dst_row0) * P.ld + col;
+        const long long col = P.cols ? (long long)oc.ci * P.ny + yv
+                                     : (long long)oc.x + (long long)P.nx * (yv + (long long)P.ny * oc.z);
+        const long long orow = P.slot ? (long long)P.slot[rk] : (long long)(dd - P.dst_row0);
+        float* out = P.dst + orow * P.ld + col;
         const float v = (float)S.acc[xx][yy][dl] * sc;
         *out = P.accumulate ? *out + v : v;
     }
@@ -430,6 +536,20 @@ cudaError_t launch_brick_sources(const ScatterParams& P, const ScatterTables& T,
                                  cudaStream_t s) {
     dim3 grid(P.n_bricks, (T.n_crystals + kScWarps - 1) / kScWarps);
     brick_sources_kernel<<<grid, kScThreads, 0, s>>>(P, T.n_crystals, brick_sources);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_scatter_transfer(const ScatterParams& P, const DevGeometry& G, const ScatterTables& T,
+                                    const float4* vbar, int n_anchors, void* K, bool k_bf16, long long ldk,
+                                    long long anchor_stride, cudaStream_t s) {
+    if (P.rank1 <= P.rank0 || T.n_crystals <= 0 || n_anchors <= 0) return cudaSuccess;
+    dim3 grid((P.rank1 - P.rank0 + 127) / 128, std::min(T.n_crystals, 65535));
+    if (k_bf16)
+        scatter_transfer_kernel<__nv_bfloat16><<<grid, 128, 0, s>>>(P, G, T, vbar, n_anchors,
+                                                                   static_cast<__nv_bfloat16*>(K), ldk, anchor_stride);
+    else
+        scatter_transfer_kernel<float><<<grid, 128, 0, s>>>(P, G, T, vbar, n_anchors, static_cast<float*>(K), ldk,
+                                                            anchor_stride);
     return cudaGetLastError();
 }
 

@@ -65,6 +65,43 @@ class ScatterOptions(ctypes.Structure):
 
 SCATTER_PARTS = {"crystal": 1, "collimator": 2, "both": 3}
 
+
+class SurrogateOptions(ctypes.Structure):
+    """sm_surrogate_options (include/sysmat_b200.h)."""
+    _fields_ = [("sp", ctypes.c_int * 3), ("parts", ctypes.c_int), ("train_frac", ctypes.c_float),
+                ("holdout_frac", ctypes.c_float), ("val_frac", ctypes.c_float), ("tol", ctypes.c_float),
+                ("anchors", ctypes.c_int * 3), ("network", ctypes.c_int), ("layers", ctypes.c_int),
+                ("width", ctypes.c_int), ("freqs", ctypes.c_int), ("emb", ctypes.c_int), ("steps", ctypes.c_int),
+                ("batch", ctypes.c_int), ("lr", ctypes.c_float), ("seed", ctypes.c_uint64)]
+
+    @staticmethod
+    def make(**kw) -> "SurrogateOptions":
+        o = SurrogateOptions()
+        lib().sm_surrogate_options_default(ctypes.byref(o))
+        for k, v in kw.items():
+            if k in ("sp", "anchors"):
+                for i in range(3):
+                    getattr(o, k)[i] = int(v[i])
+            elif k == "parts":
+                o.parts = SCATTER_PARTS[v] if isinstance(v, str) else int(v)
+            else:
+                setattr(o, k, v)
+        return o
+
+
+class SurrogateStats(ctypes.Structure):
+    """sm_surrogate_stats (include/sysmat_b200.h)."""
+    _fields_ = [(n, ctypes.c_double) for n in ("ms_total", "ms_pairs", "ms_exact_subsets", "ms_baseline", "ms_transfer",
+                                               "ms_train", "ms_correct", "ms_verify", "ms_recompute",
+                                               "ms_collimator")] + \
+               [(n, ctypes.c_int) for n in ("n_train_columns", "n_holdout_columns", "n_val_columns", "rows_corrected",
+                                            "rows_recomputed")] + \
+               [(n, ctypes.c_double) for n in ("holdout_median", "holdout_p90", "holdout_max",
+                                               "baseline_holdout_median", "final_loss")]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
 _lib = None
 _f32p = ctypes.POINTER(ctypes.c_float)
 _i64p = ctypes.POINTER(ctypes.c_int64)
@@ -112,6 +149,27 @@ PROTOTYPES = {
     "sm_scatter_compute": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(ScatterOptions), ctypes.c_int, _vp,
                                           ctypes.c_int64, ctypes.c_int, _vp, _vp, ctypes.c_int, ctypes.c_int,
                                           ctypes.c_int, _vp, ctypes.c_int64, ctypes.c_int, _vp]),
+    "sm_scatter_subset": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(ScatterOptions), ctypes.c_int, _vp, ctypes.c_int64,
+                                         _i32p, ctypes.c_int, _i32p, ctypes.c_int, _vp, ctypes.c_int64, _vp]),
+    "sm_scatter_transfer": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(ScatterOptions), ctypes.c_int, _vp, ctypes.c_int,
+                                           _vp, ctypes.c_int64, _vp]),
+    "sm_surrogate_options_default": (None, [ctypes.POINTER(SurrogateOptions)]),
+    "sm_scatter_surrogate": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(SurrogateOptions), ctypes.c_int, _vp,
+                                            ctypes.c_int64, _vp, ctypes.c_int64, _f32p, _i32p,
+                                            ctypes.POINTER(SurrogateStats), _vp]),
+    "sm_surrogate_columns": (ctypes.c_int, [_vp, ctypes.POINTER(SurrogateOptions), _i32p, ctypes.POINTER(ctypes.c_int),
+                                            ctypes.POINTER(ctypes.c_int)]),
+    "sm_surrogate_net_create": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                               ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                               ctypes.c_uint64, ctypes.POINTER(_vp)]),
+    "sm_surrogate_net_layout": (ctypes.c_int, [_vp, _i64p, _i64p]),
+    "sm_surrogate_net_get": (ctypes.c_int, [_vp, _f32p]),
+    "sm_surrogate_net_set": (ctypes.c_int, [_vp, _f32p]),
+    "sm_surrogate_net_loss_grad": (ctypes.c_int, [_vp, _i32p, _i32p, ctypes.c_int, _f32p, _f32p, ctypes.c_int64,
+                                                  ctypes.POINTER(ctypes.c_double), _f32p]),
+    "sm_surrogate_net_adam": (ctypes.c_int, [_vp, ctypes.c_float]),
+    "sm_surrogate_net_predict": (ctypes.c_int, [_vp, _i32p, ctypes.c_int, _f32p]),
+    "sm_surrogate_net_destroy": (ctypes.c_int, [_vp]),
     "sm_scatter_legacy": (ctypes.c_int, [ctypes.c_int, _f32p, _f32p, _f32p, _f32p, _f32p, ctypes.c_char_p,
                                          ctypes.c_char_p, _f32p, ctypes.c_int]),
 }
@@ -314,6 +372,67 @@ class Geometry:
                                         int(ld), 1, _vp(stream)))
         return None
 
+    def scatter_subset(self, pe_ptr: int, rows: Sequence[int], out_ptr: int, cols=None, ld: Optional[int] = None,
+                       rotation: int = 0, sp=(1, 1, 1), parts="crystal", pe_ld: Optional[int] = None,
+                       stream: int = 0):
+        """Exact scatter of the listed rows (distinct) into device ``out_ptr``:
+        every voxel (``cols`` None, row i at out[i * ld + v]) or the voxel
+        y-columns (x, z) = cols[c] (out[i * ld + c * ny + y]).  Device pointers;
+        queued on ``stream``."""
+        opt = ScatterOptions.make(sp, SCATTER_PARTS[parts] if isinstance(parts, str) else parts)
+        V = self.nx * self.ny * self.nz
+        r = np.ascontiguousarray(rows, dtype=np.int32)
+        c = None if cols is None else np.ascontiguousarray(cols, dtype=np.int32).reshape(-1, 2)
+        width = V if c is None else c.shape[0] * self.ny
+        ld = width if ld is None else int(ld)
+        _check(lib().sm_scatter_subset(self.ctx.handle, self.handle, ctypes.byref(opt), int(rotation),
+                                       _vp(int(pe_ptr)) if pe_ptr else None, int(V if pe_ld is None else pe_ld),
+                                       r.ctypes.data_as(_i32p), int(r.size),
+                                       None if c is None else c.ctypes.data_as(_i32p), 0 if c is None else int(c.shape[0]),
+                                       _vp(int(out_ptr)), ld, _vp(stream)))
+
+    def scatter_transfer(self, vbar_ptr: int, k_ptr: int, n_anchors: int = 1, ldk: Optional[int] = None,
+                         rotation: int = 0, sp=(1, 1, 1), stream: int = 0):
+        """Crystal-scatter transfer matrices K[a][d][s] into device ``k_ptr`` for
+        the device float32 [n_anchors][N][4] arrival points ``vbar_ptr``
+        (fractional voxel indices, w > 0 in use); queued on ``stream``."""
+        opt = ScatterOptions.make(sp, 1)
+        _check(lib().sm_scatter_transfer(self.ctx.handle, self.handle, ctypes.byref(opt), int(rotation),
+                                         _vp(int(vbar_ptr)), int(n_anchors), _vp(int(k_ptr)),
+                                         int(self.n_crystals if ldk is None else ldk), _vp(stream)))
+
+    def scatter_surrogate(self, pe_ptr: int, out_ptr: int, options: Optional["SurrogateOptions"] = None,
+                          rotation: int = 0, ld: Optional[int] = None, pe_ld: Optional[int] = None,
+                          stream: int = 0, **kw) -> dict:
+        """Crystal (+ collimator) scatter sysmat [N][V] into device ``out_ptr``
+        through the surrogate (physics baseline, learned correction, exact
+        re-check and recompute); ``pe_ptr`` the rotation's device PE sysmat.
+        Returns the run's statistics plus ``row_error`` (held-out error per
+        row) and ``row_state`` (0 baseline, 1 corrected, 2 recomputed)."""
+        o = options if options is not None else SurrogateOptions.make(**kw)
+        V = self.nx * self.ny * self.nz
+        st = SurrogateStats()
+        err = np.zeros(self.n_crystals, dtype=np.float32)
+        state = np.zeros(self.n_crystals, dtype=np.int32)
+        _check(lib().sm_scatter_surrogate(self.ctx.handle, self.handle, ctypes.byref(o), int(rotation),
+                                          _vp(int(pe_ptr)), int(V if pe_ld is None else pe_ld), _vp(int(out_ptr)),
+                                          int(V if ld is None else ld), _fptr(err), state.ctypes.data_as(_i32p),
+                                          ctypes.byref(st), _vp(stream)))
+        out = st.as_dict()
+        out["row_error"] = err
+        out["row_state"] = state
+        return out
+
+    def surrogate_columns(self, options: Optional["SurrogateOptions"] = None, **kw):
+        """(train, holdout): the (x, z) voxel columns a surrogate run computes exactly."""
+        o = options if options is not None else SurrogateOptions.make(**kw)
+        nt, nh = ctypes.c_int(0), ctypes.c_int(0)
+        _check(lib().sm_surrogate_columns(self.handle, ctypes.byref(o), None, ctypes.byref(nt), ctypes.byref(nh)))
+        xz = np.zeros((nt.value + nh.value, 2), dtype=np.int32)
+        _check(lib().sm_surrogate_columns(self.handle, ctypes.byref(o), xz.ctypes.data_as(_i32p), ctypes.byref(nt),
+                                          ctypes.byref(nh)))
+        return xz[:nt.value], xz[nt.value:]
+
     def record_hits(self, rows: Sequence[int], voxels: Sequence[int], rotation: int = 0,
                     opts: Optional[PeOptions] = None) -> np.ndarray:
         """Per-ray hit records of entries (rows[i], voxels[i]); shape (n, rays, words)."""
@@ -402,6 +521,63 @@ def gemm_bf16(m: int, n: int, k: int, a: int, a_strides, b: int, b_strides, c: i
                               int(b_strides[0]), int(b_strides[1]), _vp(c), int(ldc), float(alpha),
                               _vp(row_scale) if row_scale else None, _vp(bias) if bias else None, 1 if accumulate else 0,
                               int(n_tile), _vp(error) if error else None, _vp(stream)))
+
+
+class SurrogateNet:
+    """The surrogate's coordinate MLP alone (sm_surrogate_net_*): parameters,
+    loss and gradient of a batch, Adam steps and predictions, host buffers."""
+
+    def __init__(self, ctx: "Context", n_crystals: int, grid, layers: int = 6, width: int = 256, freqs: int = 16,
+                 emb: int = 64, seed: int = 1):
+        self.ctx = ctx
+        self.n_crystals = int(n_crystals)
+        self.layers = int(layers)
+        h = _vp()
+        _check(lib().sm_surrogate_net_create(ctx.handle, self.n_crystals, int(grid[0]), int(grid[1]), int(grid[2]),
+                                             self.layers, int(width), int(freqs), int(emb), int(seed),
+                                             ctypes.byref(h)))
+        self.handle = h
+        n = ctypes.c_int64(0)
+        offs = np.zeros(2 * self.layers + 3, dtype=np.int64)
+        _check(lib().sm_surrogate_net_layout(self.handle, ctypes.byref(n), offs.ctypes.data_as(_i64p)))
+        self.n_params = int(n.value)
+        self.offsets = offs
+
+    def get(self) -> np.ndarray:
+        out = np.zeros(self.n_params, dtype=np.float32)
+        _check(lib().sm_surrogate_net_get(self.handle, _fptr(out)))
+        return out
+
+    def set(self, params: np.ndarray):
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        if p.size != self.n_params:
+            raise SysmatError(-1, "expected %d parameters" % self.n_params)
+        _check(lib().sm_surrogate_net_set(self.handle, _fptr(p)))
+
+    def loss_grad(self, vox, col, rho: np.ndarray, wgt: np.ndarray):
+        v = np.ascontiguousarray(vox, dtype=np.int32)
+        c = np.ascontiguousarray(col, dtype=np.int32)
+        r = np.ascontiguousarray(rho, dtype=np.float32)
+        w = np.ascontiguousarray(wgt, dtype=np.float32)
+        loss = ctypes.c_double(0.0)
+        g = np.zeros(self.n_params, dtype=np.float32)
+        _check(lib().sm_surrogate_net_loss_grad(self.handle, v.ctypes.data_as(_i32p), c.ctypes.data_as(_i32p), v.size,
+                                                _fptr(r), _fptr(w), r.shape[1], ctypes.byref(loss), _fptr(g)))
+        return loss.value, g
+
+    def adam(self, lr: float):
+        _check(lib().sm_surrogate_net_adam(self.handle, float(lr)))
+
+    def predict(self, vox) -> np.ndarray:
+        v = np.ascontiguousarray(vox, dtype=np.int32)
+        out = np.zeros((self.n_crystals, v.size), dtype=np.float32)
+        _check(lib().sm_surrogate_net_predict(self.handle, v.ctypes.data_as(_i32p), v.size, _fptr(out)))
+        return out
+
+    def close(self):
+        if self.handle:
+            lib().sm_surrogate_net_destroy(self.handle)
+            self.handle = None
 
 
 def scatter_legacy(parts: str, collimator, detector, image, physics, pe: np.ndarray, geo_crystal: Optional[str],

@@ -221,6 +221,27 @@ int sm_scatter_compute(sm_context* ctx, const sm_geometry* geo, const sm_scatter
                        const uint32_t* collimator_bitmap, int bitmaps_on_device, int row0, int row1, float* dst,
                        int64_t ld, int dst_on_device, void* stream);
 
+/* Exact scatter on a subset of entries, device buffers: the detector rows
+ * rows[0..n_rows) (host list, distinct) against either every voxel (cols
+ * NULL: dst[i * ld + v]) or the voxel y-columns whose (x, z) are the host
+ * pairs cols[2c], cols[2c + 1] (dst[i * ld + c * ny + y]).  The same kernels
+ * and results as sm_scatter_compute on those entries; used to re-check and
+ * recompute rows of the scatter surrogate.  Returns once the work is queued
+ * on `stream`. */
+int sm_scatter_subset(sm_context* ctx, const sm_geometry* geo, const sm_scatter_options* opt, int rotation,
+                      const float* pe, int64_t ld_pe, const int32_t* rows, int n_rows, const int32_t* cols,
+                      int n_cols, float* dst, int64_t ld, void* stream);
+
+/* Crystal-scatter transfer matrices, device buffers: for each anchor
+ * a < n_anchors, K[(a * N + d) * ldk + s] = the crystal-scatter sysmat entry of
+ * detector d per unit PE of source crystal s when the photon arrives from the
+ * point vbar[4 (a N + s) .. + 2] (fractional voxel indices x, y, z;
+ * vbar[4 (a N + s) + 3] > 0 marks a source in use, else K = 0).  The same
+ * scatter terms as sm_scatter_compute (scatter points of opt->sp); the
+ * scatter surrogate's physics baseline.  Queued on `stream`. */
+int sm_scatter_transfer(sm_context* ctx, const sm_geometry* geo, const sm_scatter_options* opt, int rotation,
+                        const float* vbar, int n_anchors, float* K, int64_t ldk, void* stream);
+
 /* The reference's three `scatter` host entry points in one:
  *   parts 3: ScatterGen_RayTracing_CircularHole/scatter.h:4-5 (geo_crystal, geo_collimator)
  *   parts 1: ScatterGen_Crystal/scatter.h:4 (collimator table may be NULL; geo_crystal)
@@ -245,6 +266,91 @@ int sm_scatter_legacy(int parts, float* parameter_Collimator, float* parameter_D
 int sm_gemm_bf16(int m, int n, int k, const void* a, int64_t a_ms, int64_t a_ks, const void* b, int64_t b_ns,
                  int64_t b_ks, float* c, int64_t ldc, float alpha, const float* row_scale, const float* bias,
                  int accumulate, int n_tile, int* error, void* stream);
+
+/* ---- scatter surrogate ------------------------------------------------------------ */
+/* No reference counterpart.  The crystal-scatter sysmat from a physics
+ * baseline plus a learned correction, verified against the exact kernels:
+ *  1. exact crystal scatter on a seeded train_frac of the voxel y-columns
+ *     (x, z) and, separately, on a seeded holdout_frac of them, every row;
+ *  2. baseline B[d][v] = sum_a w_a(v) sum_s K_a[d][s] PE[s][v]: transfer
+ *     matrices K_a (sm_scatter_transfer) at an anchors[0] x [1] x [2] grid,
+ *     each source evaluated at the PE-weighted centroid of its voxels under
+ *     the anchor's trilinear weight w_a, contracted on the tensor cores;
+ *  3. (network != 0) a coordinate MLP rho(d, v) = g(d) . h(v) (Fourier
+ *     features of the voxel, `freqs` per axis; `layers` x `width`; crystal
+ *     embedding of `emb`) trained by Adam on log(S / B) of the train columns
+ *     (minus a val_frac share kept for validation), weighted by (S / rms_d)^2;
+ *     row d uses B exp(rho) where that lowers its validation error, else B;
+ *  4. each row's relative L2 error is estimated from exactly computed columns
+ *     the prediction did not use (the held-out ones; for rows without the
+ *     correction also the train ones): the sampled squared error scaled to
+ *     the whole row, over the norm of the predicted row; rows above `tol` are
+ *     recomputed exactly (all voxels);
+ *  5. the exact train and held-out entries are written in place of the
+ *     prediction; parts & 2 adds the exact collimator scatter.
+ * pe: the rotation's PE sysmat [N][ld_pe] and dst [N][ld], device buffers.
+ * Synchronous on `stream`. */
+typedef struct sm_surrogate_options {
+    int sp[3];             /* scatter points per scatter crystal (as sm_scatter_options)       */
+    int parts;             /* 1: crystal scatter, 3: crystal + collimator                     */
+    float train_frac;      /* share of voxel columns computed exactly for training (0.05)     */
+    float holdout_frac;    /* share computed exactly for the per-row check (0.005)            */
+    float val_frac;        /* share of the train columns kept for validation (0.2)            */
+    float tol;             /* per-row relative L2 error above which a row is recomputed (0.01) */
+    int anchors[3];        /* baseline anchor grid (12, 6, 12)                                 */
+    int network;           /* 1: learned correction, 0: baseline only                         */
+    int layers, width, freqs, emb;   /* network shape (6, 256, 16, 64)                         */
+    int steps, batch;      /* Adam steps and voxels per batch (600, 512)                      */
+    float lr;              /* Adam step size (2e-3)                                           */
+    uint64_t seed;
+} sm_surrogate_options;
+
+typedef struct sm_surrogate_stats {
+    double ms_total;       /* phases: */
+    double ms_pairs;       /* the crystal pair table shared by every exact and transfer step  */
+    double ms_exact_subsets, ms_baseline, ms_transfer /* part of ms_baseline */, ms_train, ms_correct, ms_verify,
+        ms_recompute, ms_collimator;
+    int n_train_columns, n_holdout_columns, n_val_columns;
+    int rows_corrected;    /* rows that use the learned correction                         */
+    int rows_recomputed;   /* rows over tol on the held-out columns, recomputed exactly    */
+    double holdout_median, holdout_p90, holdout_max;     /* per-row held-out error before recompute */
+    double baseline_holdout_median;                       /* ... of the baseline alone            */
+    double final_loss;     /* training loss at the last step                                */
+} sm_surrogate_stats;
+
+void sm_surrogate_options_default(sm_surrogate_options* opt);
+/* row_error (host, N floats, may be NULL): each row's held-out relative L2
+ * error before recompute; row_state (host, N, may be NULL): 0 predicted by the
+ * baseline, 1 predicted with the learned correction, 2 recomputed exactly. */
+int sm_scatter_surrogate(sm_context* ctx, const sm_geometry* geo, const sm_surrogate_options* opt, int rotation,
+                         const float* pe, int64_t ld_pe, float* dst, int64_t ld, float* row_error, int32_t* row_state,
+                         sm_surrogate_stats* stats, void* stream);
+/* The seeded voxel y-columns a run with these options computes exactly:
+ * n_train train columns then n_holdout held-out ones, as (x, z) pairs in xz
+ * (host, 2 (n_train + n_holdout) ints; NULL returns the counts only). */
+int sm_surrogate_columns(const sm_geometry* geo, const sm_surrogate_options* opt, int32_t* xz, int* n_train,
+                         int* n_holdout);
+
+/* The network alone, for training checks: host buffers, synchronous.
+ * Parameters are one fp32 vector: for l < layers W_l [width][in_l] and b_l
+ * [width] (in_0 = 6 freqs), then E [N][emb], P [width][emb], b_P [width];
+ * offsets[2 * layers + 3] gives each block's start. */
+typedef struct sm_surrogate_net sm_surrogate_net;
+int sm_surrogate_net_create(sm_context* ctx, int n_crystals, int nx, int ny, int nz, int layers, int width, int freqs,
+                            int emb, uint64_t seed, sm_surrogate_net** out);
+int sm_surrogate_net_layout(const sm_surrogate_net* net, int64_t* n_params, int64_t* offsets);
+int sm_surrogate_net_get(sm_surrogate_net* net, float* params);
+int sm_surrogate_net_set(sm_surrogate_net* net, const float* params);
+/* loss = sum_{d, j} wgt[d][col[j]] (rho_hat(d, vox[j]) - rho[d][col[j]])^2 / (N B)
+ * and its gradient (n_params floats) for a batch of B voxels; rho and wgt
+ * are [N][ld] host arrays. */
+int sm_surrogate_net_loss_grad(sm_surrogate_net* net, const int32_t* vox, const int32_t* col, int B, const float* rho,
+                               const float* wgt, int64_t ld, double* loss, float* grad);
+/* One Adam step (b1 0.9, b2 0.999, eps 1e-8) with the last gradient. */
+int sm_surrogate_net_adam(sm_surrogate_net* net, float lr);
+/* out[d][j] = rho_hat(d, vox[j]), [N][n] host. */
+int sm_surrogate_net_predict(sm_surrogate_net* net, const int32_t* vox, int n, float* out);
+int sm_surrogate_net_destroy(sm_surrogate_net* net);
 
 /* Diagnostic: evaluate the tracer's ray primitives on the current device for
  * n argument rows (host arrays).  kind 0: chord through a box (12 floats:

@@ -225,3 +225,48 @@ def test_scatter_small_full_size_sampled_vs_oracle(ctx):
     ref = oracle_py.oracle_scatter_entries(p, "crystal", rows, vox, bc, pe, sp=(2, 4, 2))
     ref = ref + oracle_py.oracle_scatter_entries(p, "collimator", rows, vox, bh, None)
     check_values(out[rows, vox], ref, "scatter_small")
+
+
+# ---- subsets: the surrogate's re-check and recompute path ---------------------------
+
+def test_subset_rows_and_columns_match_full_matrix(ctx):
+    """Row-list and voxel-column modes give exactly the corresponding entries
+    of the full matrix (same kernels, same per-entry sums)."""
+    import torch
+    p, z = load_scatter_golden("mid")
+    g = sysmat_b200.Geometry(ctx, p)
+    nx, ny, nz = p.grid
+    N, V = p.n_crystals, p.n_voxels
+    d_pe = torch.from_numpy(z["pe"]).cuda()
+    full = g.scatter(pe=z["pe"], sp=(1, 2, 1), parts="both")
+    rng = np.random.default_rng(11)
+    rows = rng.choice(N, 45, replace=False)
+    cols = np.stack([rng.integers(0, nx, 13), rng.integers(0, nz, 13)], 1)
+    # rows x all voxels, caller's order kept
+    out = torch.full((rows.size, V), float("nan"), device="cuda")
+    g.scatter_subset(d_pe.data_ptr(), rows, out.data_ptr(), sp=(1, 2, 1), parts="both")
+    torch.cuda.synchronize()
+    assert np.array_equal(out.cpu().numpy(), full[rows])
+    # rows x voxel columns (repeated columns allowed)
+    cols = np.concatenate([cols, cols[:2]])
+    out = torch.full((rows.size, cols.shape[0] * ny), float("nan"), device="cuda")
+    g.scatter_subset(d_pe.data_ptr(), rows, out.data_ptr(), cols=cols, sp=(1, 2, 1), parts="both")
+    torch.cuda.synchronize()
+    got = out.cpu().numpy().reshape(rows.size, cols.shape[0], ny)
+    ys = np.arange(ny)
+    vox = cols[:, 0][:, None] + nx * (ys[None, :] + ny * cols[:, 1][:, None])     # [c][y]
+    assert np.array_equal(got, full[rows][:, vox])
+    g.close()
+
+
+def test_subset_rejects_repeated_rows_and_bad_columns(ctx):
+    import torch
+    p, z = load_scatter_golden("tiny")
+    g = sysmat_b200.Geometry(ctx, p)
+    d_pe = torch.from_numpy(z["pe"]).cuda()
+    out = torch.zeros((4, p.n_voxels), device="cuda")
+    with pytest.raises(sysmat_b200.SysmatError):
+        g.scatter_subset(d_pe.data_ptr(), [1, 2, 1], out.data_ptr())
+    with pytest.raises(sysmat_b200.SysmatError):
+        g.scatter_subset(d_pe.data_ptr(), [1, 2], out.data_ptr(), cols=[(p.grid[0], 0)])
+    g.close()
