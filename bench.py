@@ -393,6 +393,8 @@ def run_ours(args, world, rank, local):
             line["scatter"] = run_scatter(args, ctx, dev)
         if world == 1 and args.sweep_steps > 0:
             line["sweep"] = run_sweep(args, ctx, dev)
+        if world == 1 and args.surrogate_steps > 0:
+            line["surrogate"] = run_surrogate(args, ctx, dev)
         print(json.dumps(line))
     geo.close()
     ctx.close()
@@ -486,6 +488,69 @@ def run_scatter(args, ctx, dev):
 
 
 # ---------------------------------------------------------------------------
+# Scatter surrogate (scatter_large: 2048 x 131072) against the all-exact matrix
+# ---------------------------------------------------------------------------
+
+def run_surrogate(args, ctx, dev):
+    """Crystal + collimator scatter of scatter_large: all exact, then through
+    the surrogate with the learned correction (the configured MLP) and without
+    it (baseline only); wall time of each on the device (CUDA events around the
+    whole call, PE resident in HBM) and each output row's true relative L2
+    error against the all-exact matrix."""
+    import torch
+    import sysmat_b200
+    p = pe_workload(args.surrogate_workload)
+    g = sysmat_b200.Geometry(ctx, p)
+    N, V = p.n_crystals, p.n_voxels
+    sp = tuple(args.scatter_points)
+    stream = torch.cuda.Stream(device=dev)
+    d_pe = torch.zeros((N, V), dtype=torch.float32, device=dev)
+    exact = torch.zeros((N, V), dtype=torch.float32, device=dev)
+    out = torch.zeros((N, V), dtype=torch.float32, device=dev)
+    with torch.cuda.stream(stream):
+        g.pe(opts=g.options(sv=(1, 1, 1), sc=(2, 4, 2)), out=d_pe.data_ptr(), stream=stream.cuda_stream)
+    stream.synchronize()
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            r = fn()
+            e1.record(stream)
+        stream.synchronize()
+        return e0.elapsed_time(e1) / 1e3, r
+
+    t_exact, _ = timed(lambda: g.scatter(pe=d_pe.data_ptr(), sp=sp, parts="both", out=exact.data_ptr(),
+                                         stream=stream.cuda_stream))
+    den = exact.double().pow(2).sum(1).sqrt().clamp_min(1e-300)
+    res = {"workload": "%s [%d x %d]: scatter_small's collimator and 2 x 32 x 32 crystals, image %dx%dx%d voxels of "
+                       "1 mm; crystal + collimator scatter, %dx%dx%d scatter points"
+                       % ((args.surrogate_workload, N, V) + tuple(p.grid) + sp),
+           "exact_s": t_exact, "exact_entries_per_s": N * V / t_exact, "variants": {}}
+    for name, kw in (("network", dict(network=1)), ("baseline_only", dict(network=0))):
+        opts = sysmat_b200.SurrogateOptions.make(sp=sp, parts=3, **kw)
+        for i in range(args.surrogate_steps):
+            t, st = timed(lambda: g.scatter_surrogate(d_pe.data_ptr(), out.data_ptr(), options=opts,
+                                                      stream=stream.cuda_stream))
+        err = ((out.double() - exact.double()).pow(2).sum(1).sqrt() / den).cpu().numpy()
+        kept = st["row_state"] != 2
+        stats = {k: v for k, v in st.items() if k not in ("row_error", "row_state")}
+        res["variants"][name] = {
+            "seconds": t, "speedup_vs_exact": t_exact / t, "entries_per_s": N * V / t,
+            "rows_recomputed": int(st["rows_recomputed"]), "rows_corrected": int(st["rows_corrected"]),
+            "true_row_error": {"median": float(np.median(err)), "p90": float(np.quantile(err, 0.9)),
+                               "p99": float(np.quantile(err, 0.99)), "max": float(err.max()),
+                               "frac_above_tol": float((err > opts.tol).mean()),
+                               "verified_rows_median": float(np.median(err[kept])) if kept.any() else 0.0},
+            "options": {"train_frac": opts.train_frac, "holdout_frac": opts.holdout_frac, "tol": opts.tol,
+                        "anchors": list(opts.anchors), "network": opts.network,
+                        "mlp": [opts.layers, opts.width, opts.freqs, opts.emb], "steps": opts.steps},
+            "stats": stats}
+    g.close()
+    return res
+
+
+# ---------------------------------------------------------------------------
 # Batched design sweep: 64 seeded geometries in one persistent graph launch
 # ---------------------------------------------------------------------------
 
@@ -563,6 +628,9 @@ def main():
     ap.add_argument("--scatter-steps", type=int, default=1, help="timed runs of the exact scatter (0 skips it)")
     ap.add_argument("--scatter-points", type=int, nargs=3, default=[2, 4, 2])
     ap.add_argument("--sweep-steps", type=int, default=1, help="timed runs of the batched sweep (0 skips it)")
+    ap.add_argument("--surrogate-steps", type=int, default=1,
+                    help="timed runs of the scatter surrogate (0 skips it)")
+    ap.add_argument("--surrogate-workload", default="scatter_large")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     if args.impl == "reference":

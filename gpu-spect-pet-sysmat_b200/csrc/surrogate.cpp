@@ -32,7 +32,7 @@ uint32_t morton2(int x, int z) {
 }
 
 struct Timer {
-    cudaEvent_t e[10];
+    cudaEvent_t e[12];
     int n = 0;
     cudaStream_t s;
     explicit Timer(cudaStream_t st) : s(st) {
@@ -304,17 +304,15 @@ int scatter_surrogate(const sm_geometry* geo, const sm_surrogate_options& o, flo
     SM_CUDA(launch_gather_columns(d_dst, ld, N, static_cast<const int2*>(dcols.p), n_tr + n_ho, nx, ny, dB, ldy, s));
     const int t2 = tm.mark();
     // baseline error estimate per row: every exactly computed column samples it
-    std::vector<double> tr_e2, tr_q2, ho_e2, ho_q2, pn2, dummy;
+    std::vector<double> tr_e2, tr_q2, ho_e2, ho_q2, dummy;
     SM_TRY(row_sums(dB, ldy, dY, ldy, N, n_trc, s, &tr_e2, &tr_q2));
     SM_TRY(row_sums(dB + n_trc, ldy, dY + n_trc, ldy, N, n_hoc, s, &ho_e2, &ho_q2));
-    SM_TRY(row_sums(d_dst, ld, d_dst, ld, N, V, s, &dummy, &pn2));
-    std::vector<double> est(N);
-    for (int d = 0; d < N; ++d) est[d] = row_estimate(tr_e2[d] + ho_e2[d], n_tr + n_ho, nx * nz, pn2[d]);
-    S.baseline_holdout_median = quantile(est, 0.5);
 
     // ---- 3. learned correction ----
     int t3 = t2, t4 = t2;
     std::vector<float> gate_host;
+    std::vector<double> val_e2;      // squared error of the corrected prediction on the validation columns
+    int n_val_lines_used = 0;
     if (o.network) {
         // validation lines: a seeded val_frac share of the train lines
         std::vector<int> line_idx(n_tr);
@@ -367,6 +365,7 @@ int scatter_surrogate(const sm_geometry* geo, const sm_surrogate_options& o, flo
                                         static_cast<const int*>(dcolvox.p), bcol, bvox, s));
             SM_CUDA(cudaMemsetAsync(net.loss, 0, sizeof(double), s));
             SM_TRY(net.forward_backward(bvox, bcol, Bsz, rho, wgt, n_trc, s));
+            if (it == 0) SM_CUDA(cudaMemcpyAsync(&S.first_loss, net.loss, sizeof(double), cudaMemcpyDeviceToHost, s));
             // warm-up over the first 5 %, then cosine decay
             const double f = (double)it / std::max(1, o.steps - 1);
             const double warm = std::min(1.0, (it + 1) / std::max(1.0, 0.05 * o.steps));
@@ -389,15 +388,26 @@ int scatter_surrogate(const sm_geometry* geo, const sm_surrogate_options& o, flo
         DevBuf dgate;
         SM_TRY(upload(dgate, ones, s, "gate"));
         SM_TRY(net.predict(static_cast<const int*>(dvalvox.p), nv, vP, nv, static_cast<const float*>(dgate.p), s));
-        std::vector<double> e_net, e_base;
-        SM_TRY(row_errors(vP, nv, vY, nv, N, nv, s, &e_net));
-        SM_TRY(row_errors(vB, nv, vY, nv, N, nv, s, &e_base));
-        std::vector<float> gate(N, 0.0f);
+        std::vector<double> e_base, q;
+        SM_TRY(row_sums(vP, nv, vY, nv, N, nv, s, &val_e2, &q));
+        SM_TRY(row_sums(vB, nv, vY, nv, N, nv, s, &e_base, &q));
+        n_val_lines_used = n_val_lines;
+        // matrix gate: the correction must lower the mean relative squared error of
+        // the rows on the validation columns by a fifth; row gate: the same per row
+        double rel_net = 0.0, rel_base = 0.0;
         for (int d = 0; d < N; ++d)
-            if (e_net[d] < 0.9 * e_base[d]) {   // a clear gain on the validation columns
-                gate[d] = 1.0f;
-                ++S.rows_corrected;
+            if (q[d] > 0.0) {
+                rel_net += val_e2[d] / q[d];
+                rel_base += e_base[d] / q[d];
             }
+        S.val_gain = rel_base > 0.0 ? 1.0 - rel_net / rel_base : 0.0;
+        std::vector<float> gate(N, 0.0f);
+        if (rel_net < 0.81 * rel_base)
+            for (int d = 0; d < N; ++d)
+                if (val_e2[d] < 0.81 * e_base[d]) {
+                    gate[d] = 1.0f;
+                    ++S.rows_corrected;
+                }
         SM_CUDA(cudaMemcpyAsync(dgate.p, gate.data(), sizeof(float) * N, cudaMemcpyHostToDevice, s));
         gate_host = gate;
         if (S.rows_corrected > 0) {
@@ -413,45 +423,16 @@ int scatter_surrogate(const sm_geometry* geo, const sm_surrogate_options& o, flo
         t4 = tm.mark();
     }
 
-    // ---- 4. per-row check ----
-    // rows with the learned correction: the held-out columns alone (the
-    // train columns fitted it and chose it); baseline rows: every exactly
-    // computed column (the baseline used none of them)
+    // corrected rows: squared error on the held-out columns; with the validation
+    // columns (not fitted; they chose the correction) they sample those rows
+    std::vector<double> c_e2;
     if (S.rows_corrected > 0) {
-        std::vector<double> c_e2, c_q2, c_n2;
+        std::vector<double> c_q2;
         SM_TRY(row_sums(dB + n_trc, ldy, dY + n_trc, ldy, N, n_hoc, s, &c_e2, &c_q2));
-        SM_TRY(row_sums(d_dst, ld, d_dst, ld, N, V, s, &dummy, &c_n2));
-        for (int d = 0; d < N; ++d)
-            if (gate_host[d] > 0.0f) est[d] = row_estimate(c_e2[d], n_ho, nx * nz, c_n2[d]);
     }
-    const std::vector<double>& ho_err = est;
-    S.holdout_median = quantile(ho_err, 0.5);
-    S.holdout_p90 = quantile(ho_err, 0.9);
-    S.holdout_max = *std::max_element(ho_err.begin(), ho_err.end());
-    std::vector<int> redo;
-    for (int d = 0; d < N; ++d)
-        if (!(ho_err[d] <= o.tol)) redo.push_back(d);
-    S.rows_recomputed = (int)redo.size();
-    if (row_error)
-        for (int d = 0; d < N; ++d) row_error[d] = (float)ho_err[d];
-    if (row_state) {
-        for (int d = 0; d < N; ++d) row_state[d] = gate_host.empty() ? 0 : (gate_host[d] > 0.0f ? 1 : 0);
-        for (int d : redo) row_state[d] = 2;
-    }
-    // exact entries replace the prediction where they exist
+    // exact entries replace the prediction where they exist; the collimator part is exact everywhere
     SM_CUDA(launch_scatter_columns(dY, ldy, N, static_cast<const int2*>(dcols.p), n_tr + n_ho, nx, ny, d_dst, ld, s));
     const int t5 = tm.mark();
-
-    // ---- 5. exact recompute of the rows over tolerance ----
-    if (!redo.empty()) {
-        ExactSpec spec;
-        spec.rows = &redo;
-        spec.rows_in_place = true;
-        spec.pairs = d_pairs;
-        spec.pairs_order = &order_all;
-        SM_TRY(exact_scatter(geo, o.sp, 1, angle, d_pe, ld_pe, nullptr, nullptr, spec, d_dst, ld, s));
-    }
-    const int t6 = tm.mark();
     if (o.parts & 2) {
         ExactSpec spec;
         spec.row0 = 0;
@@ -459,7 +440,45 @@ int scatter_surrogate(const sm_geometry* geo, const sm_surrogate_options& o, flo
         spec.accumulate = true;
         SM_TRY(exact_scatter(geo, o.sp, 2, angle, nullptr, 0, nullptr, nullptr, spec, d_dst, ld, s));
     }
+    const int t6 = tm.mark();
+
+    // ---- 4. per-row check of the output rows ----
+    // estimate = sqrt(squared error on the sampled columns scaled to the row / squared norm of the output row);
+    // baseline rows are sampled by every exactly computed column (the baseline used none of them)
+    std::vector<double> pn2, est(N), base_est(N);
+    SM_TRY(row_sums(d_dst, ld, d_dst, ld, N, V, s, &dummy, &pn2));
+    for (int d = 0; d < N; ++d) {
+        base_est[d] = row_estimate(tr_e2[d] + ho_e2[d], n_tr + n_ho, nx * nz, pn2[d]);
+        est[d] = (!gate_host.empty() && gate_host[d] > 0.0f)
+                     ? row_estimate(c_e2[d] + val_e2[d], n_ho + n_val_lines_used, nx * nz, pn2[d])
+                     : base_est[d];
+    }
+    S.baseline_holdout_median = quantile(base_est, 0.5);
+    S.holdout_median = quantile(est, 0.5);
+    S.holdout_p90 = quantile(est, 0.9);
+    S.holdout_max = *std::max_element(est.begin(), est.end());
+    std::vector<int> redo;
+    for (int d = 0; d < N; ++d)
+        if (!(est[d] <= o.tol)) redo.push_back(d);
+    S.rows_recomputed = (int)redo.size();
+    if (row_error)
+        for (int d = 0; d < N; ++d) row_error[d] = (float)est[d];
+    if (row_state) {
+        for (int d = 0; d < N; ++d) row_state[d] = gate_host.empty() ? 0 : (gate_host[d] > 0.0f ? 1 : 0);
+        for (int d : redo) row_state[d] = 2;
+    }
     const int t7 = tm.mark();
+
+    // ---- 5. exact recompute of the rows over tolerance (every part, in place) ----
+    if (!redo.empty()) {
+        ExactSpec spec;
+        spec.rows = &redo;
+        spec.rows_in_place = true;
+        spec.pairs = d_pairs;
+        spec.pairs_order = &order_all;
+        SM_TRY(exact_scatter(geo, o.sp, o.parts, angle, d_pe, ld_pe, nullptr, nullptr, spec, d_dst, ld, s));
+    }
+    const int t8 = tm.mark();
     int base_err_flag = 0;
     SM_CUDA(cudaMemcpyAsync(&base_err_flag, err_flag.p, sizeof(int), cudaMemcpyDeviceToHost, s));
     SM_CUDA(cudaStreamSynchronize(s));
@@ -469,10 +488,10 @@ int scatter_surrogate(const sm_geometry* geo, const sm_surrogate_options& o, flo
     S.ms_baseline = tm.ms(t1, t2);
     S.ms_train = tm.ms(t2, t3);
     S.ms_correct = tm.ms(t3, t4);
-    S.ms_verify = tm.ms(t4, t5);
-    S.ms_recompute = tm.ms(t5, t6);
-    S.ms_collimator = tm.ms(t6, t7);
-    S.ms_total = tm.ms(t0, t7);
+    S.ms_verify = tm.ms(t4, t5) + tm.ms(t6, t7);
+    S.ms_collimator = tm.ms(t5, t6);
+    S.ms_recompute = tm.ms(t7, t8);
+    S.ms_total = tm.ms(t0, t8);
     if (st) *st = S;
     return SM_OK;
 }

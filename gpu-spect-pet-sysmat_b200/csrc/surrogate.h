@@ -81,7 +81,7 @@ cudaError_t launch_gather_idx(const float* in, int64_t ld_in, int N, const int* 
 
 // ---- the learned correction ---------------------------------------------------------
 // rho(d, v) = g(d) . h(v): trunk h = MLP over Fourier features of the voxel
-// centre (sin, cos of w_j c per axis, w_j = pi/2 (n/2)^(j / (F - 1)), c in
+// centre (sin, cos of w_j c per axis, w_j = pi/2 min(n/2, 8)^(j / (F - 1)), c in
 // [-1, 1]), `layers` linear layers of `width` with SiLU between them; crystal
 // branch g(d) = P e_d + b_P.  Parameters are fp32 masters with bf16 copies.
 struct NetShape {

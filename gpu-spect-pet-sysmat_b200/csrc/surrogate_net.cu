@@ -3,7 +3,10 @@
 //
 // rho(d, v) = g(d) . h(v) with
 //   h(v) = trunk over Fourier features of the voxel centre: 6 F inputs
-//          (sin, cos of w_j c, c in [-1, 1] per axis, w_j = pi/2 (n/2)^(j/(F-1))),
+//          (sin, cos of w_j c, c in [-1, 1] per axis, w_j = pi/2 r^(j/(F-1)),
+//          r = min(n/2, 8): the highest frequency spans a quarter of the
+//          field, so the learned correction stays smooth between the sparse
+//          training columns instead of inventing detail there),
 //          `layers` linear layers of `width` with SiLU between them (the last
 //          one linear);
 //   g(d) = P e_d + b_P, e_d the crystal's learned `emb`-dimensional embedding.
@@ -46,7 +49,7 @@ __global__ void fourier_kernel(const int* __restrict__ vox, int n, int nx, int n
         const int idx = axis == 0 ? ix : (axis == 1 ? iy : iz);
         const int nn = axis == 0 ? nx : (axis == 1 ? ny : nz);
         const float c = 2.0f * ((float)idx + 0.5f) / (float)nn - 1.0f;
-        const float w = 1.57079632679489662f * powf(0.5f * (float)nn, F > 1 ? (float)j / (float)(F - 1) : 0.0f);
+        const float w = 1.57079632679489662f * powf(fminf(0.5f * (float)nn, 8.0f), F > 1 ? (float)j / (float)(F - 1) : 0.0f);
         const float a = c * w;
         const __nv_bfloat16 q = __float2bfloat16((rem & 1) ? cosf(a) : sinf(a));
         out[i] = q;

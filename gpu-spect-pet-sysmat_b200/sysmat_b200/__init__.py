@@ -97,7 +97,8 @@ class SurrogateStats(ctypes.Structure):
                [(n, ctypes.c_int) for n in ("n_train_columns", "n_holdout_columns", "n_val_columns", "rows_corrected",
                                             "rows_recomputed")] + \
                [(n, ctypes.c_double) for n in ("holdout_median", "holdout_p90", "holdout_max",
-                                               "baseline_holdout_median", "final_loss")]
+                                               "baseline_holdout_median", "first_loss", "final_loss",
+                                               "val_gain")]
 
     def as_dict(self):
         return {n: getattr(self, n) for n, _ in self._fields_}

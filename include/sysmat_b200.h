@@ -280,14 +280,17 @@ int sm_gemm_bf16(int m, int n, int k, const void* a, int64_t a_ms, int64_t a_ks,
  *     features of the voxel, `freqs` per axis; `layers` x `width`; crystal
  *     embedding of `emb`) trained by Adam on log(S / B) of the train columns
  *     (minus a val_frac share kept for validation), weighted by (S / rms_d)^2;
- *     row d uses B exp(rho) where that lowers its validation error, else B;
- *  4. each row's relative L2 error is estimated from exactly computed columns
- *     the prediction did not use (the held-out ones; for rows without the
- *     correction also the train ones): the sampled squared error scaled to
- *     the whole row, over the norm of the predicted row; rows above `tol` are
- *     recomputed exactly (all voxels);
- *  5. the exact train and held-out entries are written in place of the
- *     prediction; parts & 2 adds the exact collimator scatter.
+ *     if it lowers the rows' mean relative squared error on the validation
+ *     columns by a fifth, row d uses B exp(rho) where that lowers its own
+ *     squared error there by a fifth, else B;
+ *  4. the exact train and held-out entries are written in place of the
+ *     prediction; parts & 2 adds the exact collimator scatter;
+ *  5. each output row's relative L2 error is estimated from exactly computed
+ *     columns the prediction was not fitted to (rows with the correction: the
+ *     validation and held-out ones; other rows: every one): the sampled
+ *     squared error scaled to the whole row, over the squared norm of the
+ *     output row; rows above `tol` are recomputed exactly (every part, all
+ *     voxels).
  * pe: the rotation's PE sysmat [N][ld_pe] and dst [N][ld], device buffers.
  * Synchronous on `stream`. */
 typedef struct sm_surrogate_options {
@@ -315,7 +318,8 @@ typedef struct sm_surrogate_stats {
     int rows_recomputed;   /* rows over tol on the held-out columns, recomputed exactly    */
     double holdout_median, holdout_p90, holdout_max;     /* per-row held-out error before recompute */
     double baseline_holdout_median;                       /* ... of the baseline alone            */
-    double final_loss;     /* training loss at the last step                                */
+    double first_loss, final_loss;   /* training loss at the first and the last step         */
+    double val_gain;       /* 1 - (mean relative squared validation error with the correction / without) */
 } sm_surrogate_stats;
 
 void sm_surrogate_options_default(sm_surrogate_options* opt);

@@ -5,7 +5,7 @@ cores (gpu-spect-pet-sysmat_b200/csrc/surrogate_net.cu):
 
     rho(d, v) = g(d) . h(v)
     h(v) = trunk over Fourier features of the voxel centre: for each axis with
-           n voxels, c = 2 (i + 0.5) / n - 1 and w_j = pi/2 (n/2)^(j / (F - 1)),
+           n voxels, c = 2 (i + 0.5) / n - 1 and w_j = pi/2 min(n/2, 8)^(j / (F - 1)),
            features (sin w_j c, cos w_j c) for j < F (axis-major); `layers`
            linear layers of `width`, SiLU between them, the last one linear;
     g(d) = P e_d + b_P.
@@ -66,7 +66,7 @@ def fourier(vox, grid, freqs, round_bf16=True):
         c = (2.0 * (idx[axis].astype(np.float32) + np.float32(0.5)) / np.float32(n) - np.float32(1.0)).astype(np.float32)
         j = np.arange(freqs, dtype=np.float32)
         e = j / np.float32(freqs - 1) if freqs > 1 else np.zeros(1, np.float32)
-        w = np.float32(1.57079632679489662) * np.power(np.float32(0.5 * n), e).astype(np.float32)
+        w = np.float32(1.57079632679489662) * np.power(np.float32(min(0.5 * n, 8.0)), e).astype(np.float32)
         a = (c[:, None] * w[None, :]).astype(np.float32).astype(np.float64)   # the product rounds to fp32
         feats = np.empty((vox.size, 2 * freqs))
         feats[:, 0::2] = np.sin(a)
