@@ -267,8 +267,10 @@ def run_ours(args, world, rank, local):
     stream = torch.cuda.Stream(device=dev)
     opts = geo.options()
 
+    from sysmat_b200.shard import max_over_ranks, slab_of
+
     def step(i):
-        s = (i * world + rank) % n_slabs
+        s = slab_of(i, rank, world, n_slabs)
         flush.zero_()
         geo.pe(z=(s * SLAB_Z, SLAB_Z), rows=row_range, opts=opts, out=out.data_ptr(), stream=stream.cuda_stream)
 
@@ -293,7 +295,7 @@ def run_ours(args, world, rank, local):
         with torch.cuda.stream(stream):
             t_start.record(stream)
             for i in range(args.steps):
-                s = (i * world + rank) % n_slabs
+                s = slab_of(i, rank, world, n_slabs)
                 flush.zero_()
                 starts[i].record(stream)
                 geo.pe(z=(s * SLAB_Z, SLAB_Z), rows=row_range, opts=opts, out=out.data_ptr(), stream=stream.cuda_stream)
@@ -304,13 +306,7 @@ def run_ours(args, world, rank, local):
     ctx.sync(stream.cuda_stream)
     total_ms = t_start.elapsed_time(t_end)
     kernel_ms = [a.elapsed_time(b) for a, b in zip(starts, ends)]
-    if world > 1:
-        import torch.distributed as dist
-        t = torch.tensor([total_ms, sum(kernel_ms)], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms, kernel_sum = float(t[0]), float(t[1])
-    else:
-        kernel_sum = sum(kernel_ms)
+    total_ms, kernel_sum = max_over_ranks([total_ms, sum(kernel_ms)], device=dev)
     entries_per_step = rows * slab_vox
     value = world * args.steps * entries_per_step / (total_ms / 1e3)
 
