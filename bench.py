@@ -523,6 +523,12 @@ def run_surrogate(args, ctx, dev):
                        "1 mm; crystal + collimator scatter, %dx%dx%d scatter points"
                        % ((args.surrogate_workload, N, V) + tuple(p.grid) + sp),
            "exact_s": t_exact, "exact_entries_per_s": N * V / t_exact, "variants": {}}
+    # one untimed run first: the context's memory pool then holds the workspaces
+    # (transfer matrices, pair table), as in any application that calls it again
+    g.scatter_surrogate(d_pe.data_ptr(), out.data_ptr(),
+                        options=sysmat_b200.SurrogateOptions.make(sp=sp, parts=3, network=0))
+    torch.cuda.synchronize()
+    res["warmup"] = "one untimed baseline-only run before the timed ones (workspaces mapped in the context's pool)"
     for name, kw in (("network", dict(network=1)), ("baseline_only", dict(network=0))):
         opts = sysmat_b200.SurrogateOptions.make(sp=sp, parts=3, **kw)
         for i in range(args.surrogate_steps):

@@ -3,6 +3,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdarg>
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -30,9 +31,15 @@ int fail(int code, const char* fmt, ...) {
 
 const char* last_error() { return g_err; }
 
+cudaMemPool_t& current_pool() {
+    static thread_local cudaMemPool_t pool = nullptr;
+    return pool;
+}
+
 int context_bind(sm_context* ctx) {
     if (!ctx) return fail(SM_ERR_INVALID, "null context");
     SM_CUDA(cudaSetDevice(ctx->device));
+    current_pool() = ctx->pool;
     return SM_OK;
 }
 
@@ -125,6 +132,17 @@ int sm_context_create(int device, sm_context** out) {
         return rc;
     }
     ctx->d_counters = reinterpret_cast<unsigned long long*>(reinterpret_cast<char*>(ctx->d_status) + 32);
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    if (cudaMemPoolCreate(&ctx->pool, &props) == cudaSuccess) {
+        uint64_t keep = UINT64_MAX;
+        cudaMemPoolSetAttribute(ctx->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    } else {
+        ctx->pool = nullptr;   // fall back to the device's default pool
+        cudaGetLastError();
+    }
     *out = ctx;
     return SM_OK;
 }
@@ -133,7 +151,21 @@ int sm_context_destroy(sm_context* ctx) {
     if (!ctx) return SM_OK;
     cudaSetDevice(ctx->device);
     if (ctx->d_status) cudaFree(ctx->d_status);
+    if (ctx->pool) {
+        cudaDeviceSynchronize();   // frees still queued on streams reach the pool first
+        cudaMemPoolDestroy(ctx->pool);
+        if (current_pool() == ctx->pool) current_pool() = nullptr;
+    }
     delete ctx;
+    return SM_OK;
+}
+
+int sm_context_trim(sm_context* ctx) {
+    SM_TRY(context_bind(ctx));
+    if (ctx->pool) {
+        SM_CUDA(cudaDeviceSynchronize());
+        SM_CUDA(cudaMemPoolTrimTo(ctx->pool, 0));
+    }
     return SM_OK;
 }
 

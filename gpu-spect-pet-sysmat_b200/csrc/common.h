@@ -35,12 +35,21 @@ inline int check_cuda(cudaError_t e, const char* what) {
 
 #define SM_CUDA(expr) SM_TRY(::smb::check_cuda((expr), #expr))
 
-// Stream-ordered device buffer, released on the same stream.
+// The calling thread's memory pool: the one of the context last bound on this
+// thread (context_bind), or null for the device's default pool.
+cudaMemPool_t& current_pool();
+
+// Stream-ordered device buffer from the current pool, released on the same
+// stream.  A context's pool keeps freed memory mapped (no release threshold),
+// so large workspaces freed and allocated again within or across calls do not
+// pay for unmapping and mapping at every synchronisation.
 struct DevBuf {
     void* p = nullptr;
     cudaStream_t s = nullptr;
     int alloc(size_t bytes, cudaStream_t stream, const char* what) {
         s = stream;
+        cudaMemPool_t pool = current_pool();
+        if (pool) return check_cuda(cudaMallocFromPoolAsync(&p, bytes ? bytes : 16, pool, stream), what);
         return check_cuda(cudaMallocAsync(&p, bytes ? bytes : 16, stream), what);
     }
     ~DevBuf() {

@@ -15,6 +15,7 @@ struct sm_context {
     unsigned long long* d_counters = nullptr;   // 4 x u64 inside the status block
     bool collect_counters = false;
     int64_t last_counters[4] = {0, 0, 0, 0};
+    cudaMemPool_t pool = nullptr;               // device workspaces (DevBuf), kept mapped until trimmed
 };
 
 struct sm_geometry {

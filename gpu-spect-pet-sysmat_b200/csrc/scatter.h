@@ -162,5 +162,7 @@ cudaError_t launch_scatter_transfer(const ScatterParams& P, const DevGeometry& G
                                     long long anchor_stride, cudaStream_t s);
 cudaError_t launch_scatter_main(const ScatterParams& P, const DevGeometry& G, const ScatterTables& T,
                                 cudaStream_t s);
+// Crystal kind only, for row lists of scattered detectors (voxels on the lanes); same results.
+cudaError_t launch_scatter_rows(const ScatterParams& P, const DevGeometry& G, const ScatterTables& T, cudaStream_t s);
 
 }  // namespace smb

@@ -190,7 +190,7 @@ int exact_scatter(const sm_geometry* geo, const int sp[3], int parts, float angl
                 Q.pair_col = static_cast<const int*>(pcol.p);
             }
             Q.accumulate = (written || spec.accumulate) ? 1 : 0;
-            SM_CUDA(launch_scatter_main(Q, geo->dev.view, T, s));
+            SM_CUDA(spec.rows ? launch_scatter_rows(Q, geo->dev.view, T, s) : launch_scatter_main(Q, geo->dev.view, T, s));
             written = true;
             continue;
         }
@@ -213,7 +213,9 @@ int exact_scatter(const sm_geometry* geo, const int sp[3], int parts, float angl
             Q.pair_r0 = c0;
             Q.pair_ld = c1 - c0;
             Q.accumulate = (written || spec.accumulate) ? 1 : 0;
-            SM_CUDA(launch_scatter_main(Q, geo->dev.view, T, s));
+            // scattered row lists: voxels on the lanes (same results)
+            if (spec.rows && kind == kScatterCrystal) SM_CUDA(launch_scatter_rows(Q, geo->dev.view, T, s));
+            else SM_CUDA(launch_scatter_main(Q, geo->dev.view, T, s));
         }
         written = true;
     }

@@ -494,6 +494,126 @@ __global__ void __launch_bounds__(kScThreads, 2) scatter_main_kernel(ScatterPara
     }
 }
 
+// ---- crystal scatter for scattered detector rows: voxels on the lanes ----------------------
+// The same entries and the same sums as scatter_main_kernel<crystal> (per
+// entry the terms are added in the same (source, point) order, so results are
+// bit-identical), for row lists whose 32 detectors per tile lie far apart: a
+// warp is one voxel column, its lanes the column's 32 voxels, and the tile's
+// detectors are visited in turn, so the window cull of a (source point,
+// detector) pair is uniform across the warp instead of leaving most lanes
+// idle.
+struct __align__(16) ScRowSmem {
+    KnNode kn[kKnNodes + 1];
+    double acc[kScBrickX][kScBrickY][kScTileD];
+    float4 vox[kScBrickX][kScBrickY];
+    float pe[kScBrickY][kScBrickX];
+    float scale[kScTileD];
+    Det det[kScTileD];
+    int d[kScTileD];
+    long long pc[kScTileD];                    // pair column of each detector
+};
+
+__global__ void __launch_bounds__(kScThreads, 2) scatter_rows_kernel(ScatterParams P, DevGeometry G, ScatterTables T) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    ScRowSmem& S = *reinterpret_cast<ScRowSmem*>(smem_raw);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int b = blockIdx.x % P.n_bricks;
+    const int dt = blockIdx.x / P.n_bricks;
+    const BrickCol mycol = brick_column(P, b, warp);
+    const BrickCol stcol = brick_column(P, b, tid & 7);
+    const int y0 = mycol.y0;
+
+    for (int i = tid; i < kKnNodes + 1; i += kScThreads) S.kn[i] = T.kn[i];
+    for (int i = tid; i < kScBrickX * kScBrickY * kScTileD; i += kScThreads) (&S.acc[0][0][0])[i] = 0.0;
+    {
+        const int xx = tid & 7, yy = tid >> 3;
+        const int x = stcol.x, y = y0 + yy;
+        float4 v = make_float4(0.0f, 0.0f, 0.0f, -1.0f);
+        if (stcol.valid && y < P.ny) {
+            const float3 w = voxel_world(P, (float)x, (float)y, (float)stcol.z);
+            v = make_float4(w.x, w.y, w.z, 1.0f);
+        }
+        S.vox[xx][yy] = v;
+    }
+    if (warp == 0) {
+        const int rank = P.rank0 + dt * kScTileD + lane;
+        Det D;
+        D.on = false;
+        float scale = 0.0f;
+        int d = -1;
+        if (rank < P.rank1) {
+            d = P.perm[rank];
+            scale = setup_det<kScatterCrystal>(P, G, T, d, D);
+        }
+        S.det[lane] = D;
+        S.d[lane] = d;
+        S.scale[lane] = scale;
+        S.pc[lane] = rank < P.rank1 ? (P.pair_col ? (long long)P.pair_col[rank] : (long long)(rank - P.pair_r0)) : 0;
+    }
+    __syncthreads();
+    const int n_det = min(kScTileD, P.rank1 - (P.rank0 + dt * kScTileD));
+
+    const float inv_norm = T.kn_inv_norm;
+    const float4 col0 = S.vox[warp][0];
+    const float col_ex = -P.sin_a, col_ey = P.cos_a;
+    const float col_t = (float)(min(kScBrickY, P.ny - y0) - 1) * P.vy;
+    const float4 I = S.vox[warp][lane];
+    const uint32_t* srcw = P.brick_sources + (long long)b * P.src_words;
+    for (int wd = 0; wd < P.src_words; ++wd) {
+        uint32_t bits = srcw[wd];
+        while (bits) {
+            const int s = (wd << 5) + __ffs(bits) - 1;
+            bits &= bits - 1u;
+            __syncthreads();
+            {
+                const int xx = tid & 7, yy = tid >> 3;
+                float v = 0.0f;
+                if (stcol.valid && y0 + yy < P.ny)
+                    v = __ldg(P.pe + (long long)s * P.ld_pe + stcol.x +
+                              (long long)P.nx * ((y0 + yy) + (long long)P.ny * stcol.z));
+                S.pe[yy][xx] = v;
+            }
+            __syncthreads();
+            const float my_pe = S.pe[lane][warp];
+            if (!__any_sync(0xffffffffu, my_pe != 0.0f)) continue;
+            for (int p = 0; p < T.n_points; ++p) {
+                const int q = s * T.n_points + p;
+                const float4 src = T.crystal_src[q];
+                for (int dl = 0; dl < n_det; ++dl) {
+                    const Det& D = S.det[dl];
+                    if (!D.on || s == S.d[dl]) continue;
+                    Src C;
+                    make_src_basic(D, src, C);
+                    if (!(column_max_cos(C, col0.x, col0.y, col0.z, col_ex, col_ey, 0.0f, col_t) > D.c_cut)) continue;
+                    make_src_rest(D, P.pair[(long long)q * P.pair_ld + S.pc[dl]], C);
+                    if (my_pe != 0.0f) {
+                        const float isx = (I.x - D.x) * D.cm - (I.z - D.z) * D.sm;
+                        const float isy = I.y - D.y;
+                        const float isz = (I.x - D.x) * D.sm + (I.z - D.z) * D.cm;
+                        const float t = scatter_term(P, D, C, S.kn, inv_norm, I.x, I.y, I.z, isx, isy, isz);
+                        S.acc[warp][lane][dl] += (double)(my_pe * t);
+                    }
+                }
+            }
+        }
+    }
+    __syncthreads();
+    for (int i = tid; i < n_det * kScBrickY * kScBrickX; i += kScThreads) {
+        const int xx = i & 7, yy = (i >> 3) & 31, dl = i >> 8;
+        const BrickCol oc = brick_column(P, b, xx);
+        const int yv = y0 + yy;
+        if (!oc.valid || yv >= P.ny) continue;
+        const int rk = P.rank0 + dt * kScTileD + dl;
+        const int dd = S.d[dl];
+        const long long col = P.cols ? (long long)oc.ci * P.ny + yv
+                                     : (long long)oc.x + (long long)P.nx * (yv + (long long)P.ny * oc.z);
+        const long long orow = P.slot ? (long long)P.slot[rk] : (long long)(dd - P.dst_row0);
+        float* out = P.dst + orow * P.ld + col;
+        const float v = (float)S.acc[xx][yy][dl] * S.scale[dl];
+        *out = P.accumulate ? *out + v : v;
+    }
+}
+
 }  // namespace
 
 int64_t crystal_bitmap_words(int n) {
@@ -550,6 +670,18 @@ cudaError_t launch_scatter_transfer(const ScatterParams& P, const DevGeometry& G
     else
         scatter_transfer_kernel<float><<<grid, 128, 0, s>>>(P, G, T, vbar, n_anchors, static_cast<float*>(K), ldk,
                                                             anchor_stride);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_scatter_rows(const ScatterParams& P, const DevGeometry& G, const ScatterTables& T, cudaStream_t s) {
+    const size_t smem = sizeof(ScRowSmem);
+    const long long d_tiles = (P.rank1 - P.rank0 + kScTileD - 1) / kScTileD;
+    const long long blocks = d_tiles * P.n_bricks;
+    if (blocks <= 0) return cudaSuccess;
+    if (blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+    cudaError_t e = cudaFuncSetAttribute(scatter_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    scatter_rows_kernel<<<(unsigned)blocks, kScThreads, smem, s>>>(P, G, T);
     return cudaGetLastError();
 }
 

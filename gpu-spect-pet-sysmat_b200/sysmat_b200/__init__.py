@@ -119,6 +119,7 @@ PROTOTYPES = {
     "sm_context_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(_vp)]),
     "sm_context_destroy": (ctypes.c_int, [_vp]),
     "sm_context_sync": (ctypes.c_int, [_vp, _vp]),
+    "sm_context_trim": (ctypes.c_int, [_vp]),
     "sm_geometry_create": (ctypes.c_int, [_vp, _f32p, ctypes.c_size_t, _f32p, ctypes.c_size_t, _f32p,
                                           ctypes.c_size_t, _f32p, ctypes.c_size_t, ctypes.POINTER(_vp)]),
     "sm_geometry_destroy": (ctypes.c_int, [_vp]),
@@ -248,6 +249,10 @@ class Context:
 
     def sync(self, stream: int = 0):
         _check(lib().sm_context_sync(self.handle, _vp(stream)))
+
+    def trim(self):
+        """Return the context's cached device workspaces to the device."""
+        _check(lib().sm_context_trim(self.handle))
 
     def set_counters(self, enable: bool):
         _check(lib().sm_pe_set_counters(self.handle, 1 if enable else 0))

@@ -78,6 +78,11 @@ typedef struct sm_geometry sm_geometry;
 /* Binds a CUDA device (cudaSetDevice on every call that launches work). */
 int sm_context_create(int device, sm_context** out);
 int sm_context_destroy(sm_context* ctx);
+/* Device workspaces of a context's calls come from its own memory pool, which
+ * keeps freed memory mapped for the next call (no unmapping at every
+ * synchronisation).  sm_context_trim returns that memory to the device;
+ * sm_context_destroy does too. */
+int sm_context_trim(sm_context* ctx);
 /* Waits for `stream` and reports any device-side status raised by kernels of
  * this context since the last check (e.g. SM_ERR_CAPACITY). */
 int sm_context_sync(sm_context* ctx, void* stream);
