@@ -225,3 +225,44 @@ def test_trained_network_against_the_method_without_it(ctx):
     assert res[1]["median"] <= 0.01 and res[1]["frac_above_3tol"] <= 0.03, report
     assert res[0]["corrected"] == 0, report
     assert res[1]["final_loss"] < res[1]["first_loss"], report
+
+
+def test_transfer_at_a_voxel_reproduces_its_exact_column(ctx):
+    """sm_scatter_transfer evaluates the exact kernel's scatter terms: with
+    every source arriving from voxel v, sum_s K[d][s] PE[s][v] is the exact
+    crystal-scatter column v (up to fp32 summation order)."""
+    import torch
+    p, z = load_scatter_golden("mid")
+    g = sysmat_b200.Geometry(ctx, p)
+    nx, ny, nz = p.grid
+    N = p.n_crystals
+    exact = g.scatter(pe=z["pe"], sp=SP, parts="crystal")
+    pe = torch.from_numpy(z["pe"]).cuda().double()
+    rng = np.random.default_rng(3)
+    for v in rng.choice(p.n_voxels, 6, replace=False):
+        x, y, zz = v % nx, (v // nx) % ny, v // (nx * ny)
+        vb = torch.zeros((2, N, 4), device="cuda")       # two anchors: the voxel, and none (w = 0)
+        vb[0, :, 0], vb[0, :, 1], vb[0, :, 2], vb[0, :, 3] = float(x), float(y), float(zz), 1.0
+        K = torch.full((2, N, N), float("nan"), device="cuda")
+        g.scatter_transfer(vb.data_ptr(), K.data_ptr(), n_anchors=2, sp=SP)
+        torch.cuda.synchronize()
+        col = (K[0].double() @ pe[:, int(v)]).cpu().numpy()
+        ref = exact[:, int(v)].astype(np.float64)
+        assert np.all(K[1].cpu().numpy() == 0.0)
+        scale = np.abs(ref).max()
+        np.testing.assert_allclose(col, ref, rtol=1e-5, atol=1e-6 * scale)
+    g.close()
+
+
+def test_surrogate_rejects_bad_options(ctx):
+    import torch
+    p, z = load_scatter_golden("tiny")
+    g = sysmat_b200.Geometry(ctx, p)
+    pe = torch.from_numpy(z["pe"]).cuda()
+    out = torch.zeros((p.n_crystals, p.n_voxels), device="cuda")
+    for kw in (dict(train_frac=0.0), dict(train_frac=0.6, holdout_frac=0.5), dict(tol=0.0), dict(anchors=(0, 1, 1)),
+               dict(parts=2), dict(sp=(0, 1, 1)), dict(network=1, width=100), dict(network=1, batch=4)):
+        with pytest.raises(sysmat_b200.SysmatError):
+            g.scatter_surrogate(pe.data_ptr(), out.data_ptr(), **kw)
+    g.close()
+    ctx.trim()    # cached workspaces go back to the device; later calls allocate again
