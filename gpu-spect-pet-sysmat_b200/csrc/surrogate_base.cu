@@ -250,18 +250,34 @@ __global__ void __launch_bounds__(kBaseThreads) baseline_gemm_kernel(
 }
 
 // ---- column gather / scatter, per-row error ----------------------------------------------
+// Voxel index of column j (= c * ny + y) of a y-column list.
+__device__ __forceinline__ long long column_voxel(const int2* cols, long long j, int nx, int ny) {
+    const int c = (int)(j / ny), y = (int)(j - (long long)c * ny);
+    const int2 xz = cols[c];
+    return (long long)xz.x + (long long)nx * (y + (long long)ny * xz.y);
+}
+
+// out[r][j] = full[r][voxel of column j]
 __global__ void gather_columns_kernel(const float* __restrict__ full, long long ld_full, int N, const int2* __restrict__ cols,
-                                      int n_cols, int nx, int ny, float* __restrict__ out, long long ld_out, int dir) {
+                                      int n_cols, int nx, int ny, float* __restrict__ out, long long ld_out) {
     const long long W = (long long)n_cols * ny;
     const long long total = (long long)N * W;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
         const int r = (int)(i / W);
         const long long j = i - (long long)r * W;
-        const int c = (int)(j / ny), y = (int)(j - (long long)c * ny);
-        const int2 xz = cols[c];
-        const long long v = (long long)xz.x + (long long)nx * (y + (long long)ny * xz.y);
-        if (dir == 0) out[(long long)r * ld_out + j] = full[(long long)r * ld_full + v];
-        else const_cast<float*>(full)[(long long)r * ld_full + v] = out[(long long)r * ld_out + j];
+        out[(long long)r * ld_out + j] = full[(long long)r * ld_full + column_voxel(cols, j, nx, ny)];
+    }
+}
+
+// full[r][voxel of column j] = sub[r][j]
+__global__ void scatter_columns_kernel(const float* __restrict__ sub, long long ld_sub, int N, const int2* __restrict__ cols,
+                                       int n_cols, int nx, int ny, float* __restrict__ full, long long ld_full) {
+    const long long W = (long long)n_cols * ny;
+    const long long total = (long long)N * W;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
+        const int r = (int)(i / W);
+        const long long j = i - (long long)r * W;
+        full[(long long)r * ld_full + column_voxel(cols, j, nx, ny)] = sub[(long long)r * ld_sub + j];
     }
 }
 
@@ -406,7 +422,7 @@ cudaError_t launch_gather_columns(const float* full, int64_t ld_full, int N, con
     const long long total = (long long)N * n_cols * ny;
     if (total <= 0) return cudaSuccess;
     const int blocks = (int)std::min<long long>((total + 255) / 256, 148LL * 32);
-    gather_columns_kernel<<<blocks, 256, 0, s>>>(full, ld_full, N, cols, n_cols, nx, ny, out, ld_out, 0);
+    gather_columns_kernel<<<blocks, 256, 0, s>>>(full, ld_full, N, cols, n_cols, nx, ny, out, ld_out);
     return cudaGetLastError();
 }
 
@@ -415,8 +431,7 @@ cudaError_t launch_scatter_columns(const float* sub, int64_t ld_sub, int N, cons
     const long long total = (long long)N * n_cols * ny;
     if (total <= 0) return cudaSuccess;
     const int blocks = (int)std::min<long long>((total + 255) / 256, 148LL * 32);
-    gather_columns_kernel<<<blocks, 256, 0, s>>>(full, ld_full, N, cols, n_cols, nx, ny, const_cast<float*>(sub), ld_sub,
-                                                 1);
+    scatter_columns_kernel<<<blocks, 256, 0, s>>>(sub, ld_sub, N, cols, n_cols, nx, ny, full, ld_full);
     return cudaGetLastError();
 }
 
