@@ -498,10 +498,16 @@ __global__ void __launch_bounds__(kScThreads, 2) scatter_main_kernel(ScatterPara
 // The same entries and the same sums as scatter_main_kernel<crystal> (per
 // entry the terms are added in the same (source, point) order, so results are
 // bit-identical), for row lists whose 32 detectors per tile lie far apart: a
-// warp is one voxel column, its lanes the column's 32 voxels, and the tile's
-// detectors are visited in turn, so the window cull of a (source point,
-// detector) pair is uniform across the warp instead of leaving most lanes
-// idle.
+// warp is one voxel column; per source point one lane per detector runs the
+// column's window cull, then the (passing detector, voxel with PE != 0) pairs
+// are spread over the 32 lanes, so lanes are not left idle by detectors that
+// cull or voxels the source does not see.
+// Position of the n-th (from 0) set bit of m; m must have more than n set bits.
+__device__ __forceinline__ int nth_set_bit(unsigned m, int n) {
+    for (int i = 0; i < n; ++i) m &= m - 1u;
+    return __ffs(m) - 1;
+}
+
 struct __align__(16) ScRowSmem {
     KnNode kn[kKnNodes + 1];
     double acc[kScBrickX][kScBrickY][kScTileD];
@@ -557,7 +563,6 @@ __global__ void __launch_bounds__(kScThreads, 2) scatter_rows_kernel(ScatterPara
     const float4 col0 = S.vox[warp][0];
     const float col_ex = -P.sin_a, col_ey = P.cos_a;
     const float col_t = (float)(min(kScBrickY, P.ny - y0) - 1) * P.vy;
-    const float4 I = S.vox[warp][lane];
     const uint32_t* srcw = P.brick_sources + (long long)b * P.src_words;
     for (int wd = 0; wd < P.src_words; ++wd) {
         uint32_t bits = srcw[wd];
@@ -574,25 +579,41 @@ __global__ void __launch_bounds__(kScThreads, 2) scatter_rows_kernel(ScatterPara
                 S.pe[yy][xx] = v;
             }
             __syncthreads();
-            const float my_pe = S.pe[lane][warp];
-            if (!__any_sync(0xffffffffu, my_pe != 0.0f)) continue;
+            const unsigned live = __ballot_sync(0xffffffffu, S.pe[lane][warp] != 0.0f);
+            if (!live) continue;
+            const int n_live = __popc(live);
             for (int p = 0; p < T.n_points; ++p) {
                 const int q = s * T.n_points + p;
                 const float4 src = T.crystal_src[q];
-                for (int dl = 0; dl < n_det; ++dl) {
+                // window cull of the column, one detector per lane
+                bool pass = false;
+                if (lane < n_det) {
+                    const Det& D = S.det[lane];
+                    if (D.on && s != S.d[lane]) {
+                        Src C;
+                        make_src_basic(D, src, C);
+                        pass = column_max_cos(C, col0.x, col0.y, col0.z, col_ex, col_ey, 0.0f, col_t) > D.c_cut;
+                    }
+                }
+                const unsigned pmask = __ballot_sync(0xffffffffu, pass);
+                if (!pmask) continue;
+                // (passing detector, live voxel) pairs spread over the lanes; each pair once per point
+                const int n_items = __popc(pmask) * n_live;
+                for (int base = 0; base < n_items; base += 32) {
+                    const int item = base + lane;
+                    if (item >= n_items) continue;
+                    const int k = item / n_live, jj = item - k * n_live;
+                    const int dl = nth_set_bit(pmask, k), j = nth_set_bit(live, jj);
                     const Det& D = S.det[dl];
-                    if (!D.on || s == S.d[dl]) continue;
                     Src C;
                     make_src_basic(D, src, C);
-                    if (!(column_max_cos(C, col0.x, col0.y, col0.z, col_ex, col_ey, 0.0f, col_t) > D.c_cut)) continue;
                     make_src_rest(D, P.pair[(long long)q * P.pair_ld + S.pc[dl]], C);
-                    if (my_pe != 0.0f) {
-                        const float isx = (I.x - D.x) * D.cm - (I.z - D.z) * D.sm;
-                        const float isy = I.y - D.y;
-                        const float isz = (I.x - D.x) * D.sm + (I.z - D.z) * D.cm;
-                        const float t = scatter_term(P, D, C, S.kn, inv_norm, I.x, I.y, I.z, isx, isy, isz);
-                        S.acc[warp][lane][dl] += (double)(my_pe * t);
-                    }
+                    const float4 Iv = S.vox[warp][j];
+                    const float isx = (Iv.x - D.x) * D.cm - (Iv.z - D.z) * D.sm;
+                    const float isy = Iv.y - D.y;
+                    const float isz = (Iv.x - D.x) * D.sm + (Iv.z - D.z) * D.cm;
+                    const float t = scatter_term(P, D, C, S.kn, inv_norm, Iv.x, Iv.y, Iv.z, isx, isy, isz);
+                    S.acc[warp][j][dl] += (double)(S.pe[j][warp] * t);
                 }
             }
         }
