@@ -74,3 +74,31 @@ def test_pegen_and_scattergen_files(tmp_path):
     np.testing.assert_allclose(sc, c.astype(np.float64) + h, rtol=1e-6, atol=0)
     g.close()
     ctx.close()
+
+
+@pytest.mark.gpu
+def test_scattergen_surrogate_flag(tmp_path):
+    """`-surrogate TOL`: the same files, the crystal part through the scatter
+    surrogate (exact collimator part, exact recompute of rows over TOL)."""
+    p = configs.tiny(seed=4, rotated=True)
+    p.write_dat(str(tmp_path))
+    assert run("PEGen_CircularHole", ["-cuda", "0"], tmp_path).returncode == 0
+    N, V = p.n_crystals, p.n_voxels
+    assert run("ScatterGen_CircularHole", [], tmp_path).returncode == 0
+    exact = np.fromfile(tmp_path / shift_name("Scatter_SysMat", p), np.float32).reshape(2, N, V)
+    os.remove(tmp_path / shift_name("Scatter_SysMat", p))
+    r = run("ScatterGen_CircularHole", ["-surrogate", "0.01"], tmp_path)
+    assert r.returncode == 0, r.stderr
+    assert "rows recomputed" in r.stdout
+    sur = np.fromfile(tmp_path / shift_name("Scatter_SysMat", p), np.float32).reshape(2, N, V)
+    pe = np.fromfile(tmp_path / shift_name("PE_SysMat", p), np.float32).reshape(2, N, V)
+    full = np.fromfile(tmp_path / shift_name("SysMat_withScatter", p), np.float32).reshape(2, N, V)
+    assert np.isfinite(sur).all()
+    np.testing.assert_array_equal(full, pe + sur)
+    for rot in range(2):
+        num = np.sqrt(((sur[rot].astype(np.float64) - exact[rot]) ** 2).sum(1))
+        den = np.sqrt((exact[rot].astype(np.float64) ** 2).sum(1))
+        err = num[den > 0] / den[den > 0]
+        assert np.median(err) <= 0.01 and err.max() <= 0.05, (np.median(err), err.max())
+    r = run("ScatterGen_CircularHole", ["-surrogate", "0"], tmp_path)
+    assert r.returncode != 0
