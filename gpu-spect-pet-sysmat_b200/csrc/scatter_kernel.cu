@@ -347,6 +347,85 @@ __global__ void scatter_transfer_kernel(ScatterParams P, DevGeometry G, ScatterT
     }
 }
 
+// Same values as scatter_transfer_kernel, arranged for memory traffic: a CTA
+// takes 16 detectors (ranks) x 8 sources, stages the pair sums of that tile
+// once in shared memory (instead of reading them again for every pass of 8
+// anchors), and each detector's 8 consecutive sources are stored together
+// (a run of 16 or 32 bytes instead of one sector per lane).  Up to 16 scatter
+// points per crystal.
+constexpr int kTrRanks = 16, kTrSrcs = 8, kTrMaxPoints = 16;
+
+struct __align__(16) TrSmem {
+    KnNode kn[kKnNodes + 1];
+    float4 pr[kTrMaxPoints][kTrRanks][kTrSrcs];   // pair sums of the tile: [point][detector][source]
+};
+
+template <typename KT>
+__global__ void __launch_bounds__(kTrRanks * kTrSrcs) scatter_transfer_tiled_kernel(
+    ScatterParams P, DevGeometry G, ScatterTables T, const float4* __restrict__ vbar, int n_anchors,
+    KT* __restrict__ K, long long ldk, long long anchor_stride) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    TrSmem& S = *reinterpret_cast<TrSmem*>(smem_raw);
+    KnNode* kn = S.kn;
+    auto& pr = S.pr;
+    const int tid = threadIdx.x, rl = tid / kTrSrcs, sl = tid % kTrSrcs;
+    const int r0 = P.rank0 + blockIdx.x * kTrRanks, s0 = blockIdx.y * kTrSrcs;
+    const int np = T.n_points;
+    for (int i = tid; i < kKnNodes + 1; i += blockDim.x) kn[i] = T.kn[i];
+    for (int i = tid; i < np * kTrSrcs * kTrRanks; i += blockDim.x) {
+        const int r = i % kTrRanks, ss = (i / kTrRanks) % kTrSrcs, p = i / (kTrRanks * kTrSrcs);
+        const int rank = r0 + r, src = s0 + ss;
+        float4 v = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (rank < P.rank1 && src < T.n_crystals) {
+            const long long col = P.pair_col ? (long long)P.pair_col[rank] : (long long)(rank - P.pair_r0);
+            v = P.pair[(long long)(src * np + p) * P.pair_ld + col];
+        }
+        pr[p][r][ss] = v;
+    }
+    __syncthreads();
+    const int rank = r0 + rl, s = s0 + sl;
+    if (rank >= P.rank1 || s >= T.n_crystals) return;
+    const int d = P.perm[rank];
+    Det D;
+    const float scale = setup_det<kScatterCrystal>(P, G, T, d, D);
+    for (int a0 = 0; a0 < n_anchors; a0 += kMaxAnchorsPerPass) {
+        const int na = min(kMaxAnchorsPerPass, n_anchors - a0);
+        float acc[kMaxAnchorsPerPass];
+        float3 I[kMaxAnchorsPerPass], Is[kMaxAnchorsPerPass];
+        bool use[kMaxAnchorsPerPass];
+#pragma unroll
+        for (int j = 0; j < kMaxAnchorsPerPass; ++j) {
+            acc[j] = 0.0f;
+            use[j] = false;
+            if (j < na) {
+                const float4 vb = vbar[(long long)(a0 + j) * T.n_crystals + s];
+                use[j] = D.on && s != d && vb.w > 0.0f;
+                I[j] = voxel_world(P, vb.x, vb.y, vb.z);
+                Is[j] = make_float3((I[j].x - D.x) * D.cm - (I[j].z - D.z) * D.sm, I[j].y - D.y,
+                                    (I[j].x - D.x) * D.sm + (I[j].z - D.z) * D.cm);
+            }
+        }
+        bool any = false;
+#pragma unroll
+        for (int j = 0; j < kMaxAnchorsPerPass; ++j) any |= use[j];
+        if (any) {
+            for (int p = 0; p < np; ++p) {
+                Src C;
+                make_src_basic(D, T.crystal_src[s * np + p], C);
+                make_src_rest(D, pr[p][rl][sl], C);
+#pragma unroll
+                for (int j = 0; j < kMaxAnchorsPerPass; ++j)
+                    if (use[j])
+                        acc[j] += scatter_term(P, D, C, kn, T.kn_inv_norm, I[j].x, I[j].y, I[j].z, Is[j].x, Is[j].y,
+                                               Is[j].z);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < kMaxAnchorsPerPass; ++j)
+            if (j < na) K[(long long)(a0 + j) * anchor_stride + (long long)(rank - P.rank0) * ldk + s] = (KT)(acc[j] * scale);
+    }
+}
+
 struct __align__(16) ScSmem {
     KnNode kn[kKnNodes + 1];
     double acc[kScBrickX][kScBrickY][kScTileD];
@@ -684,6 +763,25 @@ cudaError_t launch_scatter_transfer(const ScatterParams& P, const DevGeometry& G
                                     const float4* vbar, int n_anchors, void* K, bool k_bf16, long long ldk,
                                     long long anchor_stride, cudaStream_t s) {
     if (P.rank1 <= P.rank0 || T.n_crystals <= 0 || n_anchors <= 0) return cudaSuccess;
+    if (T.n_points <= kTrMaxPoints && (T.n_crystals + kTrSrcs - 1) / kTrSrcs <= 65535) {
+        dim3 tg((P.rank1 - P.rank0 + kTrRanks - 1) / kTrRanks, (T.n_crystals + kTrSrcs - 1) / kTrSrcs);
+        const int smem = (int)sizeof(TrSmem);
+        cudaError_t e;
+        if (k_bf16) {
+            e = cudaFuncSetAttribute(scatter_transfer_tiled_kernel<__nv_bfloat16>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+            if (e != cudaSuccess) return e;
+            scatter_transfer_tiled_kernel<__nv_bfloat16><<<tg, kTrRanks * kTrSrcs, smem, s>>>(
+                P, G, T, vbar, n_anchors, static_cast<__nv_bfloat16*>(K), ldk, anchor_stride);
+        } else {
+            e = cudaFuncSetAttribute(scatter_transfer_tiled_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     smem);
+            if (e != cudaSuccess) return e;
+            scatter_transfer_tiled_kernel<float><<<tg, kTrRanks * kTrSrcs, smem, s>>>(
+                P, G, T, vbar, n_anchors, static_cast<float*>(K), ldk, anchor_stride);
+        }
+        return cudaGetLastError();
+    }
     dim3 grid((P.rank1 - P.rank0 + 127) / 128, std::min(T.n_crystals, 65535));
     if (k_bf16)
         scatter_transfer_kernel<__nv_bfloat16><<<grid, 128, 0, s>>>(P, G, T, vbar, n_anchors,
