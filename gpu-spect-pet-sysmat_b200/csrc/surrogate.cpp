@@ -687,6 +687,29 @@ int sm_surrogate_net_predict(sm_surrogate_net* h, const int32_t* vox, int n, flo
     return SM_OK;
 }
 
+int sm_surrogate_net_apply(sm_surrogate_net* h, const int32_t* vox, int n, const float* gate, float* inout) {
+    if (!h || !vox || !gate || !inout || n < 1) return fail(SM_ERR_INVALID, "null argument or empty list");
+    SM_TRY(context_bind(h->ctx));
+    const NetShape& s = h->net.shape;
+    const int64_t V = (int64_t)s.nx * s.ny * s.nz;
+    for (int j = 0; j < n; ++j)
+        if (vox[j] < 0 || vox[j] >= V) return fail(SM_ERR_INVALID, "voxel %d out of range", j);
+    cudaStream_t st = nullptr;
+    DevBuf idx, o, gt;
+    const size_t bytes = sizeof(float) * (size_t)s.n_crystals * n;
+    SM_TRY(idx.alloc(sizeof(int) * (size_t)n, st, "voxels"));
+    SM_TRY(o.alloc(bytes, st, "values"));
+    SM_TRY(gt.alloc(sizeof(float) * (size_t)s.n_crystals, st, "gate"));
+    SM_CUDA(cudaMemcpy(idx.p, vox, sizeof(int) * n, cudaMemcpyHostToDevice));
+    SM_CUDA(cudaMemcpy(o.p, inout, bytes, cudaMemcpyHostToDevice));
+    SM_CUDA(cudaMemcpy(gt.p, gate, sizeof(float) * s.n_crystals, cudaMemcpyHostToDevice));
+    SM_TRY(h->net.predict(static_cast<const int*>(idx.p), n, static_cast<float*>(o.p), n,
+                          static_cast<const float*>(gt.p), st));
+    SM_CUDA(cudaStreamSynchronize(st));
+    SM_CUDA(cudaMemcpy(inout, o.p, bytes, cudaMemcpyDeviceToHost));
+    return SM_OK;
+}
+
 int sm_surrogate_net_destroy(sm_surrogate_net* h) {
     if (!h) return SM_OK;
     context_bind(h->ctx);

@@ -171,6 +171,7 @@ PROTOTYPES = {
                                                   ctypes.POINTER(ctypes.c_double), _f32p]),
     "sm_surrogate_net_adam": (ctypes.c_int, [_vp, ctypes.c_float]),
     "sm_surrogate_net_predict": (ctypes.c_int, [_vp, _i32p, ctypes.c_int, _f32p]),
+    "sm_surrogate_net_apply": (ctypes.c_int, [_vp, _i32p, ctypes.c_int, _f32p, _f32p]),
     "sm_surrogate_net_destroy": (ctypes.c_int, [_vp]),
     "sm_scatter_legacy": (ctypes.c_int, [ctypes.c_int, _f32p, _f32p, _f32p, _f32p, _f32p, ctypes.c_char_p,
                                          ctypes.c_char_p, _f32p, ctypes.c_int]),
@@ -578,6 +579,16 @@ class SurrogateNet:
         v = np.ascontiguousarray(vox, dtype=np.int32)
         out = np.zeros((self.n_crystals, v.size), dtype=np.float32)
         _check(lib().sm_surrogate_net_predict(self.handle, v.ctypes.data_as(_i32p), v.size, _fptr(out)))
+        return out
+
+    def apply(self, vox, values: np.ndarray, gate) -> np.ndarray:
+        """values[d][j] * exp(gate[d] * rho(d, vox[j])): the surrogate's correction step."""
+        v = np.ascontiguousarray(vox, dtype=np.int32)
+        out = np.array(values, dtype=np.float32, order="C", copy=True)
+        g = np.ascontiguousarray(gate, dtype=np.float32)
+        if out.shape != (self.n_crystals, v.size) or g.size != self.n_crystals:
+            raise SysmatError(-1, "values must be [N][len(vox)] and gate [N]")
+        _check(lib().sm_surrogate_net_apply(self.handle, v.ctypes.data_as(_i32p), v.size, _fptr(g), _fptr(out)))
         return out
 
     def close(self):

@@ -359,6 +359,9 @@ int sm_surrogate_net_loss_grad(sm_surrogate_net* net, const int32_t* vox, const 
 int sm_surrogate_net_adam(sm_surrogate_net* net, float lr);
 /* out[d][j] = rho_hat(d, vox[j]), [N][n] host. */
 int sm_surrogate_net_predict(sm_surrogate_net* net, const int32_t* vox, int n, float* out);
+/* The surrogate's correction step: inout[d][j] *= exp(gate[d] rho_hat(d, vox[j])),
+ * [N][n] host values, gate [N] (0 leaves a row as it is). */
+int sm_surrogate_net_apply(sm_surrogate_net* net, const int32_t* vox, int n, const float* gate, float* inout);
 int sm_surrogate_net_destroy(sm_surrogate_net* net);
 
 /* Diagnostic: evaluate the tracer's ray primitives on the current device for

@@ -80,6 +80,23 @@ def test_net_prediction_matches_oracle(ctx):
     assert _rel(got, ref) <= 2e-3
 
 
+def test_net_correction_step_matches_oracle(ctx):
+    """The multiplicative correction (the GEMM's exp epilogue with a per-row
+    gate), as the pipeline applies it to the baseline."""
+    net, p, offs, shapes = _net(ctx, seed=11)
+    rng = np.random.default_rng(5)
+    vox = rng.integers(0, int(np.prod(GRID)), 37)
+    base = rng.uniform(0.5, 2.0, size=(N_SMALL, vox.size)).astype(np.float32)
+    gate = (rng.random(N_SMALL) < 0.5).astype(np.float32)
+    got = net.apply(vox, base, gate)
+    net.close()
+    rho, _ = osr.forward(p, offs, shapes, GRID, NET["freqs"], vox, round_bf16=True)
+    on = gate == 1
+    assert np.array_equal(got[~on], base[~on])
+    # the applied log-factor is the prediction (same tolerance as the prediction test)
+    assert _rel(np.log(got[on].astype(np.float64) / base[on]), rho[on]) <= 3e-3
+
+
 def test_net_adam_step_matches_oracle(ctx):
     net, p, offs, shapes = _net(ctx, seed=9)
     vox, col, rho, wgt = _batch(seed=3)
