@@ -6,7 +6,7 @@
 // Here that kernel (exact_scatter) computes a seeded subset of voxel columns,
 // a physics baseline and a learned correction predict the rest, and the exact
 // kernel re-checks held-out columns of every row and recomputes rows over
-// tolerance, so it stays both the fallback and the judge.
+// tolerance, so it stays both the fallback and the final check.
 #include <algorithm>
 #include <cmath>
 #include <cstring>

@@ -21,7 +21,7 @@ Named workloads
                32x32 crystals (60 and 66 mm) -> [2048 x 16384].
 ``scatter_large``  the same geometry with 64x64x32 voxels -> [2048 x 131072].
 
-The photoelectric mu values that BASELINE-style descriptions leave open
+The attenuation values that the workload descriptions leave open
 (plate mu_pe / mu_compton) are fixed here: tungsten 3.5 / 3.2 / 0.3 per mm,
 CZT 0.35 / 0.28 / 0.07 per mm.  Only mu_total enters the photoelectric tracer
 through the plates.
