@@ -39,6 +39,9 @@ sys.path.insert(0, os.path.join(ROOT, "gpu-spect-pet-sysmat_b200"))
 
 SLAB_Z = 4
 L2_FLUSH_BYTES = 256 << 20
+# DRAM traffic of one full pe_large slab launch (6400 x 16384 entries), read +
+# write, measured by ncu; None until measured for the current kernel.
+PE_LARGE_SLAB_DRAM_BYTES = None
 
 # FP32 operations per unit of work, counted from the tracer's source
 # (gpu-spect-pet-sysmat_b200/csrc/tracer.cuh, pe_kernel.cu): add/sub/mul/fma
@@ -126,6 +129,17 @@ def pe_workload(name: str):
     return configs.NAMED[name]()
 
 
+def workload_config(name: str, p, rows: int):
+    """The workload description both arms print (the same dict)."""
+    nx, ny, _ = p.grid
+    return {"workload": name, "crystals": rows, "voxels": p.n_voxels, "holes": p.n_holes, "plates": p.n_plates,
+            "sv": list(p.sv), "sc": list(p.sc), "rays_per_entry": p.rays_per_entry,
+            "step": "one %d-plane z-slab x all crystals (%d entries); the host arm times a seeded sample of "
+                    "entries of the same matrix per step" % (SLAB_Z, rows * nx * ny * SLAB_Z),
+            "l2": "GPU arm: L2 flushed between steps (%d MiB memset)" % (L2_FLUSH_BYTES >> 20),
+            "parallelism": "slabs sharded across ranks, no data-path collective"}
+
+
 # ---------------------------------------------------------------------------
 # CPU side: the reference's own code on the host cores
 # ---------------------------------------------------------------------------
@@ -155,6 +169,41 @@ def cpu_reference_rate(p, target_s: float, seed: int = 0, max_entries: int = 1 <
                       "OpenMP over entries, %.1f s" % (done, p.rays_per_entry, spent)}
 
 
+def error_vs_reference_fp64(p, slab_host, row0, n_rows=96, seed=3):
+    """Max and median relative error, on nonzero entries, of GPU-computed
+    entries of slab 0 against the reference's own code built with double
+    (the CPU-baseline leg's library).  Per sampled row: its 4 largest entries
+    (voxels seen through holes) and 4 random nonzero ones."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_py
+    if not oracle_py.ref_available("pe_f64"):
+        return None
+    rng = np.random.default_rng(seed)
+    rows_local = rng.choice(slab_host.shape[0], min(n_rows, slab_host.shape[0]), replace=False)
+    rows, cols = [], []
+    for r in rows_local:
+        row = slab_host[r]
+        top = np.argsort(-row)[:4]
+        nz = np.flatnonzero(row)
+        extra = rng.choice(nz, min(4, nz.size), replace=False) if nz.size else top[:0]
+        c = np.unique(np.concatenate([top, extra]))
+        rows.append(np.full(c.size, r))
+        cols.append(c)
+    rows, cols = np.concatenate(rows), np.concatenate(cols)
+    got = slab_host[rows, cols].astype(np.float64)
+    t0 = time.perf_counter()
+    ref = oracle_py.ref_pe_entries(p, rows + row0, cols, "f64")   # slab 0: column index = voxel index
+    dt = time.perf_counter() - t0
+    nz = ref != 0
+    e = np.abs(got[nz] - ref[nz]) / np.abs(ref[nz])
+    return {"median": float(np.median(e)) if e.size else None, "max": float(e.max()) if e.size else None,
+            "n_entries": int(rows.size), "n_nonzero": int(nz.sum()),
+            "zero_pattern_equal": bool(np.array_equal(got == 0, ref == 0)),
+            "vs": "fp64: the reference's kernel code built for the host with double",
+            "sample": "%d rows of slab 0, per row the 4 largest and 4 random nonzero entries; %.1f s on %d cores"
+                      % (len(rows_local), dt, os.cpu_count())}
+
+
 def run_reference_impl(args, world, rank):
     if rank != 0:
         return
@@ -179,8 +228,7 @@ def run_reference_impl(args, world, rank):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded %s geometry)" % args.workload, "impl": "reference",
-            "config": {"workload": args.workload, "crystals": p.n_crystals, "voxels": p.n_voxels,
-                       "rays_per_entry": p.rays_per_entry, "step": "bounded sample of entries"},
+            "config": workload_config(args.workload, p, p.n_crystals),
             "cpu_baseline": {"value": value, "unit": "entries/s", "cores": os.cpu_count(), "kind": "reference",
                              "sample": sample},
             "e2e": {"value": value, "unit": "entries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -322,15 +370,15 @@ def run_ours(args, world, rank, local):
     sm_max = float(peaks.get("sm_max_mhz", 1965.0))
     fp32_peak = 148 * 128 * 2 * sm_max * 1e6 / 1e12
     achieved = flops / kernel_s / 1e12
-    traffic = None
-    tpath = os.path.join(ROOT, "profiles", "pe_trace_kernel_traffic.json")
-    if os.path.exists(tpath):
-        with open(tpath) as f:
-            tr = json.load(f)
-        traffic = tr.get("bytes_per_entry", 0.0) * entries_per_step
+    # DRAM bytes (read + write) of one pe_trace_kernel launch of this step,
+    # from one ncu capture of a full pe_large slab (dram__bytes_read.sum +
+    # dram__bytes_write.sum); None for other workloads or row subsets.
+    traffic = PE_LARGE_SLAB_DRAM_BYTES if (args.workload == "pe_large" and rows == p.n_crystals) else None
 
     # End to end through the public API: tables in from host memory, slab out to pinned host memory.
     e2e = None
+    if args.e2e_steps < 0:
+        args.e2e_steps = args.steps
     if args.e2e_steps > 0:
         host = torch.empty((rows, slab_vox), dtype=torch.float32, pin_memory=True).numpy()
         barrier()
@@ -359,11 +407,7 @@ def run_ours(args, world, rank, local):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded %s geometry)" % args.workload,
-            "config": {"workload": args.workload, "crystals": rows, "voxels": p.n_voxels, "holes": p.n_holes,
-                       "plates": p.n_plates, "sv": list(p.sv), "sc": list(p.sc), "rays_per_entry": p.rays_per_entry,
-                       "step": "one %d-plane z-slab x all crystals (%d entries)" % (SLAB_Z, entries_per_step),
-                       "l2": "flushed between steps (%d MiB memset)" % (L2_FLUSH_BYTES >> 20),
-                       "parallelism": "slabs sharded across ranks, no data-path collective"},
+            "config": workload_config(args.workload, p, rows),
             "rays_per_s": value * p.rays_per_entry,
             "kernel_ms_per_step": kernel_sum / args.steps,
             "gpu_launches": args.steps,
@@ -385,6 +429,8 @@ def run_ours(args, world, rank, local):
                 line["ref_cuda"] = {"unavailable": "%s" % exc}
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_reference_rate(p, args.cpu_seconds)
+            slab0 = out.cpu().numpy()   # slab 0 of the timed rows (the counted run computed it last)
+            line["error"] = error_vs_reference_fp64(p, slab0, row_range[0])
         if world == 1 and args.scatter_steps > 0:
             line["scatter"] = run_scatter(args, ctx, dev)
         if world == 1 and args.sweep_steps > 0:
@@ -620,7 +666,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="pe_large")
-    ap.add_argument("--e2e-steps", type=int, default=1)
+    ap.add_argument("--e2e-steps", type=int, default=-1, help="end-to-end steps (default: as many as --steps)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--ref-entries", type=int, default=4096)
     ap.add_argument("--rows", type=int, default=0, help="limit the crystal rows per step (profiling runs)")

@@ -21,6 +21,7 @@ static void usage(const char* argv0) { std::printf("Usage: %s [-cuda GPU_ID] [-s
 int main(int argc, char* argv[]) {
     cli::Tables t = cli::read_params();
     cli::print_collimator(t);
+    if (!cli::check_params(t)) return 1;
     int cuda_id = 0;
     sm_pe_options opt;
     sm_pe_options_reference(&opt);

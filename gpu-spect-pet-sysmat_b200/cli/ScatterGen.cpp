@@ -108,6 +108,7 @@ static int run_surrogate(const cli::Tables& t, const cli::Grid& g, const std::ve
 int main(int argc, char* argv[]) {
     cli::Tables t = cli::read_params();
     cli::print_collimator(t);
+    if (!cli::check_params(t)) return 1;
     std::string pe_name, geo_crystal = "GeometryRelationShip_Crystal2Crystal",
                          geo_collimator = "GeometryRelationShip_Collimator2Crystal";
     int cuda_id = 0;

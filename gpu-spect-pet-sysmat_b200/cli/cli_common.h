@@ -11,36 +11,64 @@
 #include <string>
 #include <vector>
 
+#include "sysmat_b200.h"
+
 namespace cli {
 
+// The four tables in buffers of at least the reference's sizes (80000 /
+// 80000 / 100 / 100 floats, zero beyond the file), and the floats each file
+// held.  Collimator and detector files longer than 80000 floats (more than
+// 8877 holes or 6666 crystals) are read whole.
 struct Tables {
     std::vector<float> collimator = std::vector<float>(80000, 0.0f);
     std::vector<float> detector = std::vector<float>(80000, 0.0f);
     std::vector<float> image = std::vector<float>(100, 0.0f);
     std::vector<float> physics = std::vector<float>(100, 0.0f);
+    size_t n_collimator = 0, n_detector = 0, n_image = 0, n_physics = 0;
 };
 
-// Reads the table; a missing file is fatal (exit 1), a short one leaves zeros
-// as the reference's unchecked fread does, with a warning.
-inline void read_table(const char* name, std::vector<float>& out) {
+// Reads the table; a missing file is fatal (exit 1).  A file shorter than the
+// buffer leaves zeros, as the reference's fread into a zeroed buffer does;
+// whether the floats it held cover what its counts declare is checked by
+// check_params.
+inline size_t read_table(const char* name, std::vector<float>& out, bool whole) {
     FILE* f = std::fopen(name, "rb");
     if (!f) {
         std::fprintf(stderr, "ERROR: open %s\n", name);
         std::exit(1);
     }
+    if (whole && std::fseek(f, 0, SEEK_END) == 0) {
+        const long bytes = std::ftell(f);
+        if (bytes > 0 && (size_t)bytes / sizeof(float) > out.size()) out.resize((size_t)bytes / sizeof(float), 0.0f);
+        std::fseek(f, 0, SEEK_SET);
+    }
     const size_t got = std::fread(out.data(), sizeof(float), out.size(), f);
     std::fclose(f);
-    if (got < out.size())
-        std::fprintf(stderr, "warning: %s holds %zu of %zu floats; the rest are zero\n", name, got, out.size());
+    return got;
 }
 
 inline Tables read_params() {
     Tables t;
-    read_table("Params_Collimator.dat", t.collimator);
-    read_table("Params_Detector.dat", t.detector);
-    read_table("Params_Image.dat", t.image);
-    read_table("Params_Physics.dat", t.physics);
+    t.n_collimator = read_table("Params_Collimator.dat", t.collimator, true);
+    t.n_detector = read_table("Params_Detector.dat", t.detector, true);
+    t.n_image = read_table("Params_Image.dat", t.image, false);
+    t.n_physics = read_table("Params_Physics.dat", t.physics, false);
     return t;
+}
+
+// The library's table validation on what the files held (a truncated file
+// whose counts need more floats than it has is an error here, where the
+// reference silently computes with zeros).  Prints the reason and returns
+// false on failure.
+inline bool check_params(const Tables& t) {
+    int64_t info[7];
+    if (sm_tables_check(t.collimator.data(), t.n_collimator, t.detector.data(), t.n_detector, t.image.data(),
+                        t.n_image, t.physics.data(), t.n_physics, info) != SM_OK) {
+        std::fprintf(stderr, "ERROR: Params_*.dat (collimator %zu, detector %zu, image %zu floats read): %s\n",
+                     t.n_collimator, t.n_detector, t.n_image, sm_last_error());
+        return false;
+    }
+    return true;
 }
 
 inline void print_collimator(const Tables& t) {

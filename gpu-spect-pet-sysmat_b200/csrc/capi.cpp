@@ -193,6 +193,22 @@ int sm_geometry_create(sm_context* ctx, const float* collimator, size_t n_collim
     return SM_OK;
 }
 
+int sm_tables_check(const float* collimator, size_t n_collimator, const float* detector, size_t n_detector,
+                    const float* image, size_t n_image, const float* physics, size_t n_physics, int64_t out[7]) {
+    HostGeometry g;
+    SM_TRY(parse_geometry(collimator, n_collimator, detector, n_detector, image, n_image, physics, n_physics, &g));
+    if (out) {
+        out[0] = g.n_crystals;
+        out[1] = g.n_holes;
+        out[2] = g.n_plates;
+        out[3] = g.nx;
+        out[4] = g.ny;
+        out[5] = g.nz;
+        out[6] = g.n_rotations;
+    }
+    return SM_OK;
+}
+
 int sm_geometry_destroy(sm_geometry* geo) {
     if (!geo) return SM_OK;
     cudaSetDevice(geo->ctx->device);

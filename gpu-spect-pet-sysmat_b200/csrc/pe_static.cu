@@ -207,7 +207,10 @@ int validate_static(const HostGeometry& g, const sm_pe_options* opt, int row0, i
 
 // Once per device, with that device current: the device address of the array.
 // In host code g_pe_static_scratch names a host-side stand-in, never the
-// device memory, so only this address may be handed to a kernel.
+// device memory, so only this address may be handed to a kernel.  The address
+// is kept for the life of the process: after cudaDeviceReset the module is
+// loaded again and the array may move, so the entry point must not be used
+// after a reset of a device it has already run on.
 int scratch_address(int device, unsigned char** out) {
     if (device < 0 || device >= kMaxDevices) return fail(SM_ERR_DEVICE, "device %d beyond %d devices", device, kMaxDevices);
     if (!g_scratch_addr[device]) {
@@ -235,10 +238,16 @@ extern "C" int sm_pe_compute_static(const float* collimator, size_t n_collimator
     int major = 0;
     SM_CUDA(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device));
     if (major < 10) return fail(SM_ERR_DEVICE, "device %d is not sm_100 class; this build targets sm_100a", device);
+    if (opt->flags & SM_PE_AUTOTUNE)
+        return fail(SM_ERR_INVALID, "sm_pe_compute_static does not autotune (timing candidates would allocate); "
+                                    "pass tile_voxels, e.g. from an earlier sm_pe_autotune");
+    if (opt->flags != 0) return fail(SM_ERR_INVALID, "unknown option flags 0x%x", opt->flags);
     cudaPointerAttributes attr;
     SM_CUDA(cudaPointerGetAttributes(&attr, dst));
     if (attr.type != cudaMemoryTypeDevice && attr.type != cudaMemoryTypeManaged)
         return fail(SM_ERR_INVALID, "dst must be device memory of the current device");
+    if (attr.type == cudaMemoryTypeDevice && attr.device != device)
+        return fail(SM_ERR_INVALID, "dst is memory of device %d, the current device is %d", attr.device, device);
 
     unsigned char* base = nullptr;
     SM_TRY(scratch_address(device, &base));

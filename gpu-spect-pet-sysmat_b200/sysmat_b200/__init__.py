@@ -123,6 +123,8 @@ PROTOTYPES = {
     "sm_geometry_create": (ctypes.c_int, [_vp, _f32p, ctypes.c_size_t, _f32p, ctypes.c_size_t, _f32p,
                                           ctypes.c_size_t, _f32p, ctypes.c_size_t, ctypes.POINTER(_vp)]),
     "sm_geometry_destroy": (ctypes.c_int, [_vp]),
+    "sm_tables_check": (ctypes.c_int, [_f32p, ctypes.c_size_t, _f32p, ctypes.c_size_t, _f32p, ctypes.c_size_t,
+                                       _f32p, ctypes.c_size_t, _i64p]),
     "sm_geometry_info": (ctypes.c_int, [_vp, _i64p]),
     "sm_pe_options_reference": (None, [ctypes.POINTER(PeOptions)]),
     "sm_pe_compute": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(PeOptions), ctypes.c_int, ctypes.c_int, ctypes.c_int,
@@ -229,6 +231,19 @@ def PESysMatGen(parameter_Collimator, parameter_Detector, parameter_Image, dst: 
 # --------------------------------------------------------------------------
 # Status-returning API
 # --------------------------------------------------------------------------
+
+def tables_check(collimator, detector, image, physics=None) -> dict:
+    """``sm_tables_check``: the library's table validation without a device.
+    Table lengths are the arrays' sizes; raises SysmatError naming the field
+    at fault.  Returns crystals, holes, plates, grid and rotations."""
+    col, det, img = _as_f32(collimator), _as_f32(detector), _as_f32(image)
+    phy = _as_f32(physics) if physics is not None else np.zeros(0, np.float32)
+    out = np.zeros(7, np.int64)
+    _check(lib().sm_tables_check(_fptr(col), col.size, _fptr(det), det.size, _fptr(img), img.size,
+                                 _fptr(phy) if phy.size else None, phy.size, out.ctypes.data_as(_i64p)))
+    return {"crystals": int(out[0]), "holes": int(out[1]), "plates": int(out[2]),
+            "grid": (int(out[3]), int(out[4]), int(out[5])), "rotations": int(out[6])}
+
 
 class Context:
     def __init__(self, device: int = 0):

@@ -94,6 +94,12 @@ int sm_geometry_create(sm_context* ctx, const float* collimator, size_t n_collim
                        const float* detector, size_t n_detector, const float* image, size_t n_image,
                        const float* physics, size_t n_physics, sm_geometry** out);
 int sm_geometry_destroy(sm_geometry* geo);
+/* Host only, no device needed: the parse and validation of sm_geometry_create
+ * (the checks the reference's table readers never make: counts that need
+ * more floats than a table holds, e.g. a truncated Params_*.dat, plate and
+ * crystal sizes, grid).  out (may be NULL) as sm_geometry_info. */
+int sm_tables_check(const float* collimator, size_t n_collimator, const float* detector, size_t n_detector,
+                    const float* image, size_t n_image, const float* physics, size_t n_physics, int64_t out[7]);
 /* n_crystals, n_holes, n_plates, nx, ny, nz, n_rotations */
 int sm_geometry_info(const sm_geometry* geo, int64_t out[7]);
 
@@ -135,7 +141,11 @@ int sm_pe_compute(sm_context* ctx, const sm_geometry* geo, const sm_pe_options* 
  *   - Geometries whose derived tables exceed the array (about 40000 crystals
  *     with 2000 holes) are rejected with SM_ERR_CAPACITY.
  *   - The first call on a device looks up the array's device address once
- *     (set-up); make that first call before any stream capture.
+ *     (set-up); make that first call before any stream capture.  The address
+ *     is kept until the process exits: do not call this entry point after
+ *     cudaDeviceReset of a device it has already run on.
+ *   - opt->flags must be 0 (autotuning would allocate: SM_ERR_INVALID); dst
+ *     that is host memory or memory of another device is SM_ERR_INVALID.
  *   - Every call shares the one array, which keeps the previous call's
  *     contents; calls overlapping on the GPU would race, so the library runs
  *     one call at a time per process and returns only after its kernel has

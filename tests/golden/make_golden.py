@@ -14,8 +14,21 @@ small seeded geometries, and stores inputs and outputs as .npz files:
                          (crystal and collimator words), sampled (row, voxel)
                          cells, and the reference's f32 and f64 crystal- and
                          collimator-scatter values.
+* ``pe_shipped_<name>.npz`` the two geometries the reference ships as data files
+                         (``PEGen_RayTracing_CircularHole/Params_*.dat``: 5632
+                         crystals in 4 layers, one plate with 1865 holes, 64^3
+                         voxels of 2 mm; ``Param_*.dat``: one crystal outside a
+                         plate whose 4 holes have zero length, 64x64x32 voxels,
+                         60 rotations), with the reference's f32 and f64 values
+                         on sampled cells in its own mode (voxel centre, 8x16x8
+                         crystal sub-cells).  Rows are contiguous blocks spread
+                         over the detector layers; within each row the cells mix
+                         the largest entries (voxels seen through holes) with
+                         random ones.
 
-Usage: ``python tests/golden/make_golden.py`` (needs oracle/_ref built).
+Usage: ``python tests/golden/make_golden.py [pe|scatter|shipped]`` (needs
+oracle/_ref built; ``shipped`` reads the reference tree named by
+SYSMAT_REFERENCE_TREE, default /root/reference).
 """
 from __future__ import annotations
 
@@ -127,7 +140,74 @@ def prim_rays(kind: str, n: int, seed: int) -> np.ndarray:
     return np.stack(rows)
 
 
+SHIPPED_ROW_BLOCKS = {
+    # row blocks [r0, r0 + 8): layers 0, 1, 2 (32 x 16 crystals each) and layer 3 (64 x 64)
+    "params": ((0, 8), (712, 720), (1324, 1332), (3600, 3608), (5624, 5632)),
+    "param_degenerate": ((0, 1),),
+}
+
+
+def _read_table(path, n_max):
+    raw = np.fromfile(path, dtype="<f4")
+    return raw[:n_max].astype(np.float32)
+
+
+def shipped_fixture(tree: str, name: str, prefix: str):
+    """Tables of a geometry the reference ships, and the reference's own values
+    on sampled cells (reference mode)."""
+    from sysmat_b200.params import Params
+    d = os.path.join(tree, "PEGen_RayTracing_CircularHole")
+    col = _read_table(os.path.join(d, prefix + "_Collimator.dat"), 80000)
+    det = _read_table(os.path.join(d, prefix + "_Detector.dat"), 80000)
+    img = _read_table(os.path.join(d, prefix + "_Image.dat"), 100)
+    phy = _read_table(os.path.join(d, prefix + "_Physics.dat"), 100)
+    n_holes = sum(int(np.floor(col[(l + 1) * 10] + np.float32(0.001))) for l in
+                  range(int(np.floor(col[0] + np.float32(0.001)))))
+    n_crystals = int(np.floor(det[0] + np.float32(0.001)))
+    col = col[:100 + 9 * n_holes] if col.size >= 100 + 9 * n_holes else col
+    det = det[:1 + 12 * n_crystals] if det.size >= 1 + 12 * n_crystals else det
+    padded = lambda a, n: np.concatenate([a, np.zeros(max(0, n - a.size), np.float32)])  # noqa: E731
+    p = Params(padded(col, 80000), padded(det, 80000), padded(img, 100), padded(phy, 100), (1, 1, 1),
+               (8, 16, 8), "shipped_" + name)
+    rng = np.random.default_rng(zlib.crc32(("shipped_" + name).encode()))
+    rotations = (0,) if p.n_rotations == 1 else (0, p.n_rotations // 2, p.n_rotations - 1)
+    rows_all, vox_all, rot_all = [], [], []
+    for rot in rotations:
+        for r0, r1 in SHIPPED_ROW_BLOCKS[name]:
+            for row in range(r0, r1):
+                cand = rng.choice(p.n_voxels, 256, replace=False)
+                v = oracle_py.oracle_pe_entries(p, np.full(cand.size, row), cand, "fp32", rotation=rot)
+                top = cand[np.argsort(-v)[:3]]
+                nz = cand[v != 0]
+                rest = rng.choice(nz, min(3, nz.size), replace=False) if nz.size else cand[:0]
+                anyv = rng.choice(cand, 2, replace=False)
+                pick = np.unique(np.concatenate([top, rest, anyv]))
+                rows_all.append(np.full(pick.size, row))
+                vox_all.append(pick)
+                rot_all.append(np.full(pick.size, rot))
+    rows = np.concatenate(rows_all)
+    vox = np.concatenate(vox_all)
+    rot = np.concatenate(rot_all)
+    f32 = np.zeros(rows.size)
+    f64 = np.zeros(rows.size)
+    for r in rotations:
+        m = rot == r
+        f32[m] = oracle_py.ref_pe_entries(p, rows[m], vox[m], "f32", rotation=int(r))
+        f64[m] = oracle_py.ref_pe_entries(p, rows[m], vox[m], "f64", rotation=int(r))
+    np.savez_compressed(os.path.join(HERE, "pe_shipped_%s.npz" % name), collimator=col, detector=det, image=img,
+                        physics=phy, sv=np.asarray(p.sv), sc=np.asarray(p.sc), rows=rows, voxels=vox, rotation=rot,
+                        ref_f32=f32, ref_f64=f64,
+                        row_blocks=np.asarray(SHIPPED_ROW_BLOCKS[name], dtype=np.int64))
+    print("pe_shipped_%s: %d crystals, %d holes, grid %s, %d cells, nonzero %d" % (
+        name, p.n_crystals, p.n_holes, p.grid, rows.size, int((f64 != 0).sum())))
+
+
 def main():
+    if len(sys.argv) > 1 and sys.argv[1] == "shipped":
+        tree = os.environ.get("SYSMAT_REFERENCE_TREE", "/root/reference")
+        shipped_fixture(tree, "params", "Params")
+        shipped_fixture(tree, "param_degenerate", "Param")
+        return
     if len(sys.argv) > 1 and sys.argv[1] == "scatter":
         for name, (factory, rotation, n_cells) in SCATTER_CASES.items():
             scatter_fixture(name, factory, rotation, n_cells)

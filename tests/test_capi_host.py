@@ -86,3 +86,55 @@ def test_seeded_generators_are_deterministic():
     a, b = configs.pe_large(), configs.pe_large()
     assert np.array_equal(a.collimator, b.collimator)
     assert not np.array_equal(configs.pe_large(seed=2).collimator, a.collimator)
+
+
+# ---- table validation without a device (sm_tables_check) ---------------------
+
+def test_tables_check_reports_the_geometry():
+    p = configs.two_plates_small()
+    info = sysmat_b200.tables_check(p.collimator, p.detector, p.image, p.physics)
+    assert info == {"crystals": p.n_crystals, "holes": p.n_holes, "plates": 2, "grid": p.grid, "rotations": 1}
+
+
+def test_tables_check_rejects_truncated_tables():
+    p = configs.tiny()
+    n = p.n_crystals
+    with pytest.raises(sysmat_b200.SysmatError) as e:
+        sysmat_b200.tables_check(p.collimator, p.detector[:1 + 12 * (n - 3)], p.image)
+    assert e.value.code == -2 and "%d crystals need %d detector floats" % (n, 1 + 12 * n) in str(e.value)
+    with pytest.raises(sysmat_b200.SysmatError) as e:
+        sysmat_b200.tables_check(p.collimator[:100 + 9 * (p.n_holes - 1)], p.detector, p.image)
+    assert e.value.code == -2 and "holes need" in str(e.value)
+    with pytest.raises(sysmat_b200.SysmatError) as e:
+        sysmat_b200.tables_check(p.collimator, p.detector, p.image[:8])
+    assert e.value.code == -1 and "image table" in str(e.value)
+
+
+def test_tables_check_names_bad_fields():
+    p = configs.tiny()
+    det = p.detector.copy()
+    det[1 + 12 * 5 + 4] = 0.0              # crystal 5 width
+    with pytest.raises(sysmat_b200.SysmatError) as e:
+        sysmat_b200.tables_check(p.collimator, det, p.image)
+    assert "crystal 5" in str(e.value)
+    col = p.collimator.copy()
+    col[12] = -1.0                          # plate 0 thickness
+    with pytest.raises(sysmat_b200.SysmatError) as e:
+        sysmat_b200.tables_check(col, p.detector, p.image)
+    assert "plate 0" in str(e.value)
+
+
+def test_cli_rejects_a_truncated_params_file(tmp_path):
+    """The reference's CLI freads into a zeroed buffer and computes with the
+    zeros; here a Params_*.dat whose counts need more floats than it holds is
+    an error, reported before any device work."""
+    p = configs.tiny()
+    p.write_dat(str(tmp_path))
+    n = p.n_crystals
+    p.detector[:1 + 12 * (n - 2)].astype("<f4").tofile(tmp_path / "Params_Detector.dat")
+    binary = os.path.join(os.path.dirname(sysmat_b200.LIB_PATH), "..", "..", "bin", "PEGen_CircularHole")
+    import subprocess
+    r = subprocess.run([binary], cwd=tmp_path, capture_output=True, text=True, timeout=60)
+    assert r.returncode == 1
+    assert "Params_*.dat" in r.stderr and "%d crystals need" % n in r.stderr
+    assert not list(tmp_path.glob("*.sysmat"))

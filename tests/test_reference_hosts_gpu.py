@@ -1,0 +1,111 @@
+"""The reference's own CLI hosts, unmodified, linked against this library.
+
+oracle/Makefile (target ``ref-cli``) compiles the reference's
+``PEGen_RayTracing_CircularHole/PEGen_CircularHole.cpp`` and
+``ScatterGen_RayTracing_CircularHole/ScatterGen_CircularHole.cpp`` twice, with
+no source change:
+
+* ``*.sysmat_b200``: linked against libsysmat_b200.so, the way a maintainer
+  switches the reference to this library (the ``PESysMatGen`` / ``scatter``
+  drop-ins, include/sysmat_b200.h);
+* ``*.ref``: linked against the reference's own ``PESysMatGen.cu`` /
+  ``scatter.cu`` built for sm_100a.
+
+Both run in their own working directory on the same ``Params_*.dat`` and must
+write the same files: the PE sysmat with identical zero patterns and values
+within 1e-4 relative (the two implementations take the same single-precision
+hit decisions and differ only in value arithmetic), the geometry bitmaps bit
+for bit, and the scatter sysmat within the tolerance of the scatter parity
+tests (the reference's scatter kernels add with float atomics in no fixed
+order).
+"""
+import os
+import shutil
+import subprocess
+
+import numpy as np
+import pytest
+
+from helpers import rel_err
+from sysmat_b200 import configs
+
+pytestmark = pytest.mark.gpu
+
+REF_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "..", "oracle", "_ref")
+
+
+def _binary(name):
+    path = os.path.join(REF_DIR, name)
+    if not os.path.exists(path):
+        pytest.skip("%s not built (the reference tree was absent when oracle/ was built)" % name)
+    return path
+
+
+def _run(binary, cwd, args=()):
+    r = subprocess.run([binary] + list(args), cwd=cwd, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, "%s failed: %s %s" % (os.path.basename(binary), r.stdout[-2000:], r.stderr[-2000:])
+    return r
+
+
+def _shift_name(prefix, p):
+    return "%s_shift_%f_%f_%f.sysmat" % (prefix, p.image[8], p.image[9], p.image[10])
+
+
+def _pe_case():
+    """Rotated crystals, two image rotations, a shifted FOV and 6 z-planes (the
+    reference host's 4-plane slab loop ends on a 2-plane slab)."""
+    p = configs.tiny(seed=4, rotated=True)
+    p.image = p.image.copy()
+    p.image[2] = 6
+    p.image[30] = 6
+    return p
+
+
+def test_reference_pegen_host_on_library_matches_reference_build(tmp_path):
+    ours_bin = _binary("PEGen_CircularHole.sysmat_b200")
+    ref_bin = _binary("PEGen_CircularHole.ref")
+    p = _pe_case()
+    out = {}
+    for tag, binary in (("ours", ours_bin), ("ref", ref_bin)):
+        d = tmp_path / tag
+        p.write_dat(str(d))
+        _run(binary, d, ["-cuda", "0"])
+        out[tag] = np.fromfile(d / _shift_name("PE_SysMat", p), np.float32)
+    N, V = p.n_crystals, p.n_voxels
+    assert out["ours"].size == out["ref"].size == 2 * N * V
+    assert (out["ref"] != 0).sum() > 0.1 * out["ref"].size
+    assert np.array_equal(out["ours"] == 0, out["ref"] == 0)
+    err = rel_err(out["ours"], out["ref"])
+    assert err.max() <= 1e-4, err.max()
+
+
+def test_reference_scattergen_host_on_library_matches_reference_build(tmp_path):
+    ours_bin = _binary("ScatterGen_CircularHole.sysmat_b200")
+    ref_bin = _binary("ScatterGen_CircularHole.ref")
+    p = configs.scatter_mid()                  # 2 x 64 crystals, 25 holes, 8 x 8 x 6 voxels, one rotation
+    N, V = p.n_crystals, p.n_voxels
+    import sysmat_b200
+    ctx = sysmat_b200.Context(0)
+    g = sysmat_b200.Geometry(ctx, p)
+    pe = g.pe(opts=sysmat_b200.PeOptions.make((1, 1, 1), (8, 16, 8)))
+    g.close()
+    ctx.close()
+    files = {}
+    for tag, binary in (("ours", ours_bin), ("ref", ref_bin)):
+        d = tmp_path / tag
+        p.write_dat(str(d))
+        pe.astype(np.float32).tofile(d / _shift_name("PE_SysMat", p))
+        _run(binary, d, ["-cuda", "0"])
+        files[tag] = {name: (d / name).read_bytes() for name in
+                      ("GeometryRelationShip_Crystal2Crystal", "GeometryRelationShip_Collimator2Crystal")}
+        files[tag]["scatter"] = np.fromfile(d / _shift_name("Scatter_SysMat", p), np.float32)
+        files[tag]["total"] = np.fromfile(d / _shift_name("SysMat_withScatter", p), np.float32)
+    for name in ("GeometryRelationShip_Crystal2Crystal", "GeometryRelationShip_Collimator2Crystal"):
+        assert len(files["ours"][name]) > 0 and files["ours"][name] == files["ref"][name], name
+    a, b = files["ours"]["scatter"], files["ref"]["scatter"]
+    assert a.size == b.size == N * V and (b != 0).any()
+    err = rel_err(a, b)
+    assert np.median(err) <= 1e-4 and np.quantile(err, 0.99) <= 1e-3 and err.max() <= 2e-2
+    np.testing.assert_array_equal(files["ours"]["total"], pe.ravel() + a)
+    shutil.rmtree(tmp_path / "ours", ignore_errors=True)
+    shutil.rmtree(tmp_path / "ref", ignore_errors=True)
