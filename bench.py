@@ -431,6 +431,8 @@ def run_ours(args, world, rank, local):
             line["cpu_baseline"] = cpu_reference_rate(p, args.cpu_seconds)
             slab0 = out.cpu().numpy()   # slab 0 of the timed rows (the counted run computed it last)
             line["error"] = error_vs_reference_fp64(p, slab0, row_range[0])
+        if world == 1:
+            line["beam_metrics"] = run_beam_metrics(out, stream)
         if world == 1 and args.scatter_steps > 0:
             line["scatter"] = run_scatter(args, ctx, dev)
         if world == 1 and args.sweep_steps > 0:
@@ -443,6 +445,35 @@ def run_ours(args, world, rank, local):
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# Beam masks and MPXI of the resident slab (sysmat_b200.beams)
+# ---------------------------------------------------------------------------
+
+def run_beam_metrics(block, stream, reps: int = 5):
+    """sm_beam_metrics on a resident sysmat block (masks kept): HBM-bound;
+    algorithmic bytes per entry = 4 (sysmat read) + 1 (mask written) + 1
+    (mask read for MPXI).  The block (419 MB for pe_large) exceeds L2."""
+    import torch
+    from sysmat_b200 import beams
+    peaks, src = load_peaks()
+    with torch.cuda.stream(stream):
+        beams.beam_metrics(block, stream=stream)          # warm-up
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            m = beams.beam_metrics(block, stream=stream)
+        e1.record(stream)
+    stream.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    entries = block.shape[0] * block.shape[1]
+    gbs = 6.0 * entries / (ms / 1e3) / 1e9
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    return {"entries": entries, "ms": ms, "bytes_per_entry": 6, "achieved_gbs": gbs, "peak_gbs": hbm,
+            "frac": gbs / hbm, "peak_source": src, "active_rows": int((m["row_count"] > 0).sum()),
+            "mpxi_max": int(m["mpxi"].max()),
+            "timed": "row stats + int8 masks + MPXI of the resident slab 0, CUDA events, mean of %d" % reps}
 
 
 # ---------------------------------------------------------------------------

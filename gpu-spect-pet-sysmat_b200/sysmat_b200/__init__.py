@@ -137,6 +137,8 @@ PROTOTYPES = {
     "sm_pe_set_counters": (ctypes.c_int, [_vp, ctypes.c_int]),
     "sm_pe_last_counters": (ctypes.c_int, [_vp, _i64p]),
     "sm_primitive_batch": (ctypes.c_int, [ctypes.c_int, _f32p, ctypes.c_int64, _f32p]),
+    "sm_beam_metrics": (ctypes.c_int, [_vp, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_float, _vp, _vp,
+                                       _vp, _vp, ctypes.c_int64, _vp, _vp]),
     "sm_pe_autotune": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(PeOptions), ctypes.c_int, ctypes.POINTER(PeOptions),
                                       ctypes.POINTER(ctypes.c_double)]),
     "sm_pe_batch_create": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(_vp), ctypes.POINTER(PeOptions),

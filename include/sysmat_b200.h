@@ -374,6 +374,23 @@ int sm_surrogate_net_predict(sm_surrogate_net* net, const int32_t* vox, int n, f
 int sm_surrogate_net_apply(sm_surrogate_net* net, const int32_t* vox, int n, const float* gate, float* inout);
 int sm_surrogate_net_destroy(sm_surrogate_net* net);
 
+/* ---- beam masks and multiplexing of a sysmat (analysis on the device) ----------- */
+/* The reference computes these on the CPU from a memory-mapped .sysmat file
+ * (PEGen_RayTracing_CircularHole/extract_beam_prop_masks.py:52-87,
+ * compute_mpxi_3d.py:45-52).  For one rotation's block of a PE sysmat in
+ * device memory, sysmat[r * ld + v] (r < rows, v < voxels), and device
+ * outputs:
+ *   row_max[r], row_sum[r] (double), row_count[r] = size of the beam mask,
+ *   the mask of row r being sysmat[r][v] > frac * row_max[r] (the product in
+ *   single precision; threshold 1.0 when row_max[r] <= 0; the reference uses
+ *   frac = 0.05);
+ *   mask[r * ld_mask + v] (int8 0/1; may be NULL);
+ *   mpxi[v] = number of rows whose mask holds voxel v (uint32; may be NULL).
+ * Asynchronous on `stream`, on the current device.  NaN entries count as
+ * below every threshold and do not raise the maximum. */
+int sm_beam_metrics(const float* sysmat, int64_t rows, int64_t voxels, int64_t ld, float frac, float* row_max,
+                    double* row_sum, int32_t* row_count, int8_t* mask, int64_t ld_mask, uint32_t* mpxi, void* stream);
+
 /* Diagnostic: evaluate the tracer's ray primitives on the current device for
  * n argument rows (host arrays).  kind 0: chord through a box (12 floats:
  * segment in, out, box min, max), 1: chord from box entry to segment end

@@ -26,8 +26,17 @@ small seeded geometries, and stores inputs and outputs as .npz files:
                          the largest entries (voxels seen through holes) with
                          random ones.
 
-Usage: ``python tests/golden/make_golden.py [pe|scatter|shipped]`` (needs
-oracle/_ref built; ``shipped`` reads the reference tree named by
+* ``beams_reference.npz`` the reference's beam post-processing
+                         (extract_beam_prop_masks.py, compute_mpxi_3d.py) run
+                         here on a synthetic sysmat whose rows cycle through a
+                         pool: the pool, its masks, rotation 0's beam
+                         properties, MPXI and summary.
+* ``mpxi_shipped_rot000.npz`` the MPXI volume the reference ships
+                         (``beam_masks/mpxi_3d/mpxi_3d_rot_000.npy``) and the
+                         summary text its script wrote for it.
+
+Usage: ``python tests/golden/make_golden.py [pe|scatter|shipped|beams]`` (needs
+oracle/_ref built; ``shipped`` and ``beams`` read the reference tree named by
 SYSMAT_REFERENCE_TREE, default /root/reference).
 """
 from __future__ import annotations
@@ -202,7 +211,161 @@ def shipped_fixture(tree: str, name: str, prefix: str):
         name, p.n_crystals, p.n_holes, p.grid, rows.size, int((f64 != 0).sum())))
 
 
+# ---------------------------------------------------------------------------
+# Beam masks / MPXI: the reference's own post-processing scripts, run here
+# ---------------------------------------------------------------------------
+
+class _Stub:
+    """Stands in for a module the reference scripts import but this image lacks
+    (h5py, matplotlib): any attribute is another stub, calls return stubs."""
+
+    def __init__(self, name="stub"):
+        self._name = name
+
+    def __getattr__(self, item):
+        return _Stub(self._name + "." + item)
+
+    def __call__(self, *a, **k):
+        return _Stub(self._name + "()")
+
+
+class _Dataset:
+    """h5py dataset stand-in that keeps the rows the test fixture needs."""
+
+    def __init__(self, shape, dtype, keep_rows):
+        self.shape = tuple(shape)
+        self.keep = keep_rows
+        self.data = np.zeros((min(keep_rows, self.shape[0]),) + self.shape[1:], dtype)
+        self.count = 0
+
+    def resize(self, shape):
+        self.shape = tuple(shape)
+        if shape[0] > self.data.shape[0] and self.data.shape[0] < self.keep:
+            grow = np.zeros((min(self.keep, shape[0]) - self.data.shape[0],) + self.data.shape[1:], self.data.dtype)
+            self.data = np.concatenate([self.data, grow])
+
+    def __setitem__(self, idx, value):
+        row = idx[0] if isinstance(idx, tuple) else idx
+        if row < self.data.shape[0]:
+            self.data[row] = value
+
+    def __getitem__(self, idx):
+        return self.data[idx]
+
+
+class _H5File:
+    def __init__(self, path, mode="r", keep_rows=0):
+        self.path = path
+        self.sets = {}
+        self.keep_rows = keep_rows
+
+    def create_dataset(self, name, shape, maxshape=None, dtype="float32"):
+        ds = _Dataset(shape, dtype, self.keep_rows)
+        self.sets[name] = ds
+        return ds
+
+    def close(self):
+        pass
+
+
+def _pool_rows(k=29):
+    """k distinct sysmat rows of 4096 voxels: photoelectric rows of the pe_small
+    geometry (voxel centres, 2x4x2 sub-cells) from the oracle, an all-zero row
+    (threshold 1.0) and a row holding entries exactly at 0.05 * max (strict >)."""
+    p = configs.pe_small()
+    p.sv = (1, 1, 1)
+    rows = []
+    for i, crystal in enumerate(np.linspace(0, p.n_crystals - 1, k - 2).astype(int)):
+        rows.append(oracle_py.oracle_pe_entries(p, np.full(4096, crystal), np.arange(4096), "fp32").astype(np.float32))
+    rows.append(np.zeros(4096, np.float32))
+    tie = rows[5].copy()
+    mx = tie.max()
+    thr = np.float32(0.05) * mx
+    tie[::7] = thr
+    rows.append(tie)
+    return np.stack(rows)
+
+
+def beams_fixture(tree: str):
+    """Runs the reference's extract_3d_beams() (extract_beam_prop_masks.py)
+    unmodified on a synthetic 60-rotation x 5632-crystal x 4096-voxel sysmat
+    whose rows cycle through a pool, and compute_mpxi_3d.py's
+    compute_mpxi_for_rotation / summarize_mpxi on its rotation-0 masks.  Only
+    the file layer is replaced (np.memmap by a view that builds each requested
+    row from the pool; h5py by in-memory datasets; matplotlib by a stub)."""
+    import importlib.util
+    import types
+    d = os.path.join(tree, "PEGen_RayTracing_CircularHole")
+    pool = _pool_rows()
+    n_det, n_vox, n_rot = 5632, 4096, 60
+
+    class LazySysmat:
+        def __getitem__(self, sl):
+            start = sl.start
+            g = start // n_vox
+            assert sl.stop - start == n_vox and start % n_vox == 0
+            return pool[g % len(pool)]
+
+    fake_np = types.SimpleNamespace(**{k: getattr(np, k) for k in dir(np) if not k.startswith("__")})
+    fake_np.memmap = lambda *a, **k: LazySysmat()
+    files = {}
+
+    def h5file(path, mode="r"):
+        f = _H5File(path, mode, keep_rows=n_det)
+        files[os.path.basename(path)] = f
+        return f
+
+    saved = {m: sys.modules.get(m) for m in ("h5py", "matplotlib", "matplotlib.pyplot")}
+    h5 = types.ModuleType("h5py")
+    h5.File = h5file
+    mpl = types.ModuleType("matplotlib")
+    mpl.use = lambda *a, **k: None
+    plt = _Stub("matplotlib.pyplot")
+    mpl.pyplot = plt
+    sys.modules["h5py"], sys.modules["matplotlib"], sys.modules["matplotlib.pyplot"] = h5, mpl, plt
+    try:
+        spec = importlib.util.spec_from_file_location("ref_extract_beams", os.path.join(d, "extract_beam_prop_masks.py"))
+        ext = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(ext)
+        ext.np = fake_np
+        ext.extract_3d_beams()
+        spec = importlib.util.spec_from_file_location("ref_mpxi", os.path.join(d, "compute_mpxi_3d.py"))
+        mp = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(mp)
+    finally:
+        for m, v in saved.items():
+            if v is None:
+                sys.modules.pop(m, None)
+            else:
+                sys.modules[m] = v
+    masks = files["beams_masks_3d.hdf5"].sets["beam_mask"]
+    props = files["beams_properties_3d.hdf5"].sets["beam_properties"]
+    mpxi = mp.compute_mpxi_for_rotation(masks, 0)
+    summary = mp.summarize_mpxi(mpxi)
+    n_active0 = int((masks.data[:n_det].sum(axis=1) > 0).sum())
+    hist = np.asarray(summary["histogram"], dtype=np.int64)
+    np.savez_compressed(os.path.join(HERE, "beams_reference.npz"), pool=pool,
+                        pool_masks=masks.data[:len(pool)], props_rot0=props.data[:n_active0],
+                        n_active_total=np.int64(props.shape[0]), mpxi_rot0=mpxi.astype(np.uint32),
+                        summary_hist=hist, summary_scalars=np.asarray(
+                            [summary["num_voxels_sampled"], summary["num_voxels_unsampled"],
+                             summary["num_voxels_nonmultiplexed"], summary["num_voxels_multiplexed"],
+                             summary["max_mpxi"]], np.int64),
+                        summary_means=np.asarray([summary["mean_mpxi_all_voxels"], summary["mean_mpxi_sampled_voxels"],
+                                                  summary["median_mpxi_sampled_voxels"]], np.float64),
+                        dims=np.asarray([n_rot, n_det, n_vox], np.int64))
+    shipped = os.path.join(d, "beam_masks", "mpxi_3d")
+    vol = np.load(os.path.join(shipped, "mpxi_3d_rot_000.npy"))
+    text = open(os.path.join(shipped, "mpxi_3d_rot_000_summary.txt")).read()
+    np.savez_compressed(os.path.join(HERE, "mpxi_shipped_rot000.npz"), mpxi=vol, summary_text=np.asarray(text))
+    print("beams_reference: pool %d rows, active beams %d (rotation 0: %d), mpxi max %d; shipped mpxi %s %s" % (
+        len(pool), int(props.shape[0]), n_active0, int(mpxi.max()), vol.shape, vol.dtype))
+
+
 def main():
+    if len(sys.argv) > 1 and sys.argv[1] == "beams":
+        beams_fixture(os.environ.get("SYSMAT_REFERENCE_TREE", "/root/reference"))
+        return
     if len(sys.argv) > 1 and sys.argv[1] == "shipped":
         tree = os.environ.get("SYSMAT_REFERENCE_TREE", "/root/reference")
         shipped_fixture(tree, "params", "Params")
