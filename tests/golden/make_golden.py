@@ -35,8 +35,13 @@ small seeded geometries, and stores inputs and outputs as .npz files:
                          (``beam_masks/mpxi_3d/mpxi_3d_rot_000.npy``) and the
                          summary text its script wrote for it.
 
-Usage: ``python tests/golden/make_golden.py [pe|scatter|shipped|beams]`` (needs
-oracle/_ref built; ``shipped`` and ``beams`` read the reference tree named by
+* ``geometry_json_reference.npz`` the reference's json_to_dat.py and
+                         check_geometry_sanity.py run here: tables of three
+                         JSON geometries, error messages for broken ones, and
+                         the printed sanity reports.
+
+Usage: ``python tests/golden/make_golden.py [pe|scatter|shipped|beams|json]``
+(needs oracle/_ref built; ``shipped``, ``beams`` and ``json`` read the reference tree named by
 SYSMAT_REFERENCE_TREE, default /root/reference).
 """
 from __future__ import annotations
@@ -362,7 +367,103 @@ def beams_fixture(tree: str):
         len(pool), int(props.shape[0]), n_active0, int(mpxi.max()), vol.shape, vol.dtype))
 
 
+# ---------------------------------------------------------------------------
+# JSON front-end and sanity report: the reference's json_to_dat.py and
+# check_geometry_sanity.py, run here
+# ---------------------------------------------------------------------------
+
+def _strip_comments(o):
+    if isinstance(o, dict):
+        return {k: _strip_comments(v) for k, v in o.items() if not k.startswith("_comment")}
+    if isinstance(o, list):
+        return [_strip_comments(v) for v in o]
+    return o
+
+
+def geometry_json_fixture(tree: str):
+    """Tables json_to_dat.py builds from three JSON geometries (the reference's
+    annotated example without its comment keys, and two of this project's
+    seeded configurations written in the schema), the error messages it gives
+    for broken inputs, and what check_geometry_sanity.py prints for exact-size
+    tables of those geometries and of the shipped Params tables."""
+    import contextlib
+    import copy
+    import importlib.util
+    import io
+    import json
+    import tempfile
+    from sysmat_b200 import geometry_json
+    d = os.path.join(tree, "PEGen_RayTracing_CircularHole")
+
+    def load(name, fname):
+        spec = importlib.util.spec_from_file_location(name, os.path.join(d, fname))
+        m = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(m)
+        return m
+
+    j2d = load("ref_json_to_dat", "json_to_dat.py")
+    san = load("ref_sanity", "check_geometry_sanity.py")
+    cases = {"annotated": _strip_comments(json.load(open(os.path.join(d, "geometry.annotated.json")))),
+             "two_plates": geometry_json.params_to_json(configs.two_plates_small()),
+             "tiny_rot": geometry_json.params_to_json(configs.tiny(seed=4, rotated=True))}
+    out = {}
+    for name, cfg in cases.items():
+        tables = [j2d.build_param_collimator(cfg["collimator"], 10, 100), j2d.build_param_detector(cfg["detector"]),
+                  j2d.build_param_image(cfg["image"]), j2d.build_param_physics(cfg["physics"])]
+        out["json_" + name] = np.asarray(json.dumps(cfg))
+        for key, arr in zip(("collimator", "detector", "image", "physics"), tables):
+            out["%s_%s" % (key, name)] = arr
+    broken = []
+    base = cases["two_plates"]
+    edits = [("collimator", lambda c: c["collimator"]["layers"][0].pop("mu_pe")),
+             ("detector", lambda c: c["detector"]["bins"][3].pop("cy")),
+             ("collimator", lambda c: c["collimator"]["layers"][1].__setitem__("hole_count", 7)),
+             ("image", lambda c: c["image"].__setitem__("num_voxel_x", "six")),
+             ("detector", lambda c: c["detector"].__setitem__("bins", []))]
+    for section, edit in edits:
+        cfg = copy.deepcopy(base)
+        edit(cfg)
+        fn = {"collimator": lambda c: j2d.build_param_collimator(c["collimator"], 10, 100),
+              "detector": lambda c: j2d.build_param_detector(c["detector"]),
+              "image": lambda c: j2d.build_param_image(c["image"])}[section]
+        try:
+            fn(cfg)
+            msg = ""
+        except SystemExit as e:
+            msg = str(e)
+        broken.append((json.dumps(cfg), msg))
+    out["broken_json"] = np.asarray([b[0] for b in broken])
+    out["broken_msg"] = np.asarray([b[1] for b in broken])
+    shipped = np.load(os.path.join(HERE, "pe_shipped_params.npz"))
+    sanity_inputs = {name: (out["collimator_" + name], out["detector_" + name], out["image_" + name])
+                     for name in cases}
+    sanity_inputs["shipped"] = (shipped["collimator"], shipped["detector"], shipped["image"])
+    with tempfile.TemporaryDirectory() as tmp:
+        for name, (c, dt, im) in sanity_inputs.items():
+            paths = []
+            for key, arr in (("col", c), ("det", dt), ("img", im)):
+                path = os.path.join(tmp, "%s_%s.dat" % (name, key))
+                np.asarray(arr, np.float32).tofile(path)
+                paths.append(path)
+            argv = sys.argv
+            sys.argv = ["check_geometry_sanity.py", "--param_collimator", paths[0], "--param_detector", paths[1],
+                        "--param_image", paths[2]]
+            buf = io.StringIO()
+            try:
+                with contextlib.redirect_stdout(buf):
+                    san.main()
+            finally:
+                sys.argv = argv
+            out["sanity_" + name] = np.asarray(buf.getvalue())
+    np.savez_compressed(os.path.join(HERE, "geometry_json_reference.npz"), **out)
+    print("geometry_json_reference: %d geometries, %d broken inputs, %d sanity reports" % (
+        len(cases), len(broken), len(sanity_inputs)))
+
+
 def main():
+    if len(sys.argv) > 1 and sys.argv[1] == "json":
+        geometry_json_fixture(os.environ.get("SYSMAT_REFERENCE_TREE", "/root/reference"))
+        return
     if len(sys.argv) > 1 and sys.argv[1] == "beams":
         beams_fixture(os.environ.get("SYSMAT_REFERENCE_TREE", "/root/reference"))
         return
