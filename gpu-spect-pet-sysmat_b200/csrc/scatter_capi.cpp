@@ -6,6 +6,7 @@
 #include <cstdio>
 #include <cstring>
 #include <mutex>
+#include <string>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -331,6 +332,71 @@ int write_words(const char* path, const std::vector<uint32_t>& w) {
     return SM_OK;
 }
 
+// ---- geometry hashes of the bitmap files ------------------------------------
+// A bitmap file holds no record of the geometry it was computed for, so the
+// reference reuses a stale -GeoCrystal / -GeoCollimator file after the tables
+// change.  Next to each file this library writes "<file>.geohash": one line
+// naming the bitmap kind, its word count and a 64-bit FNV-1a hash of every
+// table value the bitmap depends on.  Reading a bitmap whose .geohash names
+// another geometry recomputes it (and refreshes both files); a bitmap without
+// .geohash (written by the reference) is read as the reference reads it.
+
+uint64_t fnv1a(const void* data, size_t n, uint64_t h) {
+    const unsigned char* p = static_cast<const unsigned char*>(data);
+    for (size_t i = 0; i < n; ++i) {
+        h ^= p[i];
+        h *= 0x100000001b3ULL;
+    }
+    return h;
+}
+
+// out[0]: crystal bitmap (detector records and the FOV distance);
+// out[1]: collimator bitmap (plate 0's record and holes, detector, FOV distance).
+void bitmap_hashes(const HostGeometry& g, uint64_t out[2]) {
+    const uint64_t seed = 0xcbf29ce484222325ULL;
+    const size_t n_det = 1 + 12 * (size_t)g.n_crystals;
+    uint64_t hd = fnv1a("crystal-bitmap-v1", 17, seed);
+    hd = fnv1a(g.detector.data(), sizeof(float) * n_det, hd);
+    hd = fnv1a(&g.image[11], sizeof(float), hd);
+    out[0] = hd;
+    const int h0 = holes0_of(g);
+    uint64_t hh = fnv1a("collimator-bitmap-v1", 20, seed);
+    if (g.collimator.size() >= 18) hh = fnv1a(&g.collimator[10], sizeof(float) * 8, hh);
+    hh = fnv1a(&h0, sizeof(h0), hh);
+    if (h0 > 0) hh = fnv1a(&g.collimator[100], sizeof(float) * 9 * (size_t)h0, hh);
+    hh = fnv1a(g.detector.data(), sizeof(float) * n_det, hh);
+    hh = fnv1a(&g.image[11], sizeof(float), hh);
+    out[1] = hh;
+}
+
+std::string hash_line(const char* kind, int64_t words, uint64_t hash) {
+    char buf[128];
+    std::snprintf(buf, sizeof(buf), "sysmat_b200-bitmap-v1 %s words=%lld fnv1a64=%016llx\n", kind, (long long)words,
+                  (unsigned long long)hash);
+    return buf;
+}
+
+int write_hash_file(const char* bitmap_path, const std::string& line) {
+    const std::string path = std::string(bitmap_path) + ".geohash";
+    FILE* f = std::fopen(path.c_str(), "wb");
+    if (!f) return fail(SM_ERR_IO, "cannot create %s", path.c_str());
+    const bool ok = std::fwrite(line.data(), 1, line.size(), f) == line.size();
+    std::fclose(f);
+    return ok ? SM_OK : fail(SM_ERR_IO, "short write to %s", path.c_str());
+}
+
+// 1: the .geohash file exists and names this geometry; 0: it names another
+// one; -1: there is none.
+int hash_file_matches(const char* bitmap_path, const std::string& line) {
+    const std::string path = std::string(bitmap_path) + ".geohash";
+    FILE* f = std::fopen(path.c_str(), "rb");
+    if (!f) return -1;
+    char buf[256] = {0};
+    const size_t got = std::fread(buf, 1, sizeof(buf) - 1, f);
+    std::fclose(f);
+    return (got == line.size() && std::memcmp(buf, line.data(), got) == 0) ? 1 : 0;
+}
+
 int validate_scatter(const sm_geometry* geo, const sm_scatter_options* opt, int row0, int row1) {
     for (int a = 0; a < 3; ++a)
         if (opt->sp[a] < 1 || opt->sp[a] > 16) return fail(SM_ERR_INVALID, "sp[%d] = %d must be in 1..16", a, opt->sp[a]);
@@ -404,6 +470,12 @@ int sm_scatter_bitmap_words(const sm_geometry* geo, int64_t out[2]) {
     if (!geo || !out) return fail(SM_ERR_INVALID, "null argument");
     out[0] = crystal_bitmap_words(geo->host.n_crystals);
     out[1] = collimator_bitmap_words(geo->host.n_crystals, holes0_of(geo->host));
+    return SM_OK;
+}
+
+int sm_scatter_bitmap_hashes(const sm_geometry* geo, uint64_t out[2]) {
+    if (!geo || !out) return fail(SM_ERR_INVALID, "null argument");
+    bitmap_hashes(geo->host, out);
     return SM_OK;
 }
 
@@ -541,23 +613,39 @@ int sm_scatter_legacy(int parts, float* parameter_Collimator, float* parameter_D
     const int64_t V = (int64_t)g.nx * g.ny * g.nz;
     int64_t words[2];
     sm_scatter_bitmap_words(geo, words);
+    uint64_t hashes[2];
+    bitmap_hashes(g, hashes);
     std::vector<uint32_t> bmc, bmh;
     if (parts & 1) {
         if (!geo_crystal) return fail(SM_ERR_INVALID, "crystal bitmap file name is required");
-        if ((int)std::floor(parameter_Physics[8]) == 1) {
+        const std::string line = hash_line("crystal", words[0], hashes[0]);
+        const bool compute = (int)std::floor(parameter_Physics[8]) == 1;
+        const int match = compute ? -1 : hash_file_matches(geo_crystal, line);
+        if (compute || match == 0) {
+            if (match == 0)
+                std::fprintf(stderr, "scatter: %s was computed for another geometry (%s.geohash); recomputing it\n",
+                             geo_crystal, geo_crystal);
             bmc.assign((size_t)words[0], 0u);
             SM_TRY(sm_scatter_bitmaps(ctx, geo, bmc.data(), nullptr, 0, nullptr));
             SM_TRY(write_words(geo_crystal, bmc));
+            SM_TRY(write_hash_file(geo_crystal, line));
         } else {
             SM_TRY(read_words(geo_crystal, &bmc, words[0]));
         }
     }
     if ((parts & 2) && words[1] > 0) {
         if (!geo_collimator) return fail(SM_ERR_INVALID, "collimator bitmap file name is required");
-        if ((int)std::floor(parameter_Physics[9] + 0.001f) == 1) {
+        const std::string line = hash_line("collimator", words[1], hashes[1]);
+        const bool compute = (int)std::floor(parameter_Physics[9] + 0.001f) == 1;
+        const int match = compute ? -1 : hash_file_matches(geo_collimator, line);
+        if (compute || match == 0) {
+            if (match == 0)
+                std::fprintf(stderr, "scatter: %s was computed for another geometry (%s.geohash); recomputing it\n",
+                             geo_collimator, geo_collimator);
             bmh.assign((size_t)words[1], 0u);
             SM_TRY(sm_scatter_bitmaps(ctx, geo, nullptr, bmh.data(), 0, nullptr));
             SM_TRY(write_words(geo_collimator, bmh));
+            SM_TRY(write_hash_file(geo_collimator, line));
         } else {
             SM_TRY(read_words(geo_collimator, &bmh, words[1]));
         }

@@ -151,6 +151,7 @@ PROTOTYPES = {
                                     ctypes.c_int, ctypes.c_int, _vp, _vp]),
     "sm_scatter_options_reference": (None, [ctypes.POINTER(ScatterOptions)]),
     "sm_scatter_bitmap_words": (ctypes.c_int, [_vp, _i64p]),
+    "sm_scatter_bitmap_hashes": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_uint64)]),
     "sm_scatter_bitmaps": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_int, _vp]),
     "sm_scatter_compute": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(ScatterOptions), ctypes.c_int, _vp,
                                           ctypes.c_int64, ctypes.c_int, _vp, _vp, ctypes.c_int, ctypes.c_int,
@@ -342,6 +343,12 @@ class Geometry:
     def bitmap_words(self) -> Tuple[int, int]:
         out = np.zeros(2, dtype=np.int64)
         _check(lib().sm_scatter_bitmap_words(self.handle, out.ctypes.data_as(_i64p)))
+        return int(out[0]), int(out[1])
+
+    def bitmap_hashes(self) -> Tuple[int, int]:
+        """Geometry hashes of the crystal and collimator bitmaps (the .geohash values)."""
+        out = (ctypes.c_uint64 * 2)()
+        _check(lib().sm_scatter_bitmap_hashes(self.handle, out))
         return int(out[0]), int(out[1])
 
     def scatter_bitmaps(self) -> Tuple[np.ndarray, np.ndarray]:

@@ -216,6 +216,15 @@ void sm_scatter_options_reference(sm_scatter_options* opt);
  * bits, H0 = holes of plate 0). */
 int sm_scatter_bitmap_words(const sm_geometry* geo, int64_t out[2]);
 
+/* 64-bit FNV-1a hashes of the table values each bitmap depends on: out[0]
+ * crystal bitmap (detector records, FOV distance), out[1] collimator bitmap
+ * (plate 0's record and holes, detector records, FOV distance).  The legacy
+ * scatter path keeps them in "<bitmap file>.geohash" next to the files it
+ * writes, and recomputes a bitmap whose .geohash names another geometry
+ * instead of reading it (the reference reuses such a stale file); a bitmap
+ * file without .geohash is read as the reference reads it. */
+int sm_scatter_bitmap_hashes(const sm_geometry* geo, uint64_t out[2]);
+
 /* Computes either bitmap (NULL skips it) into device (on_device != 0, async on
  * `stream`) or host buffers, bit for bit the reference's
  * geometryRelationShip_Crystal2Crystal / _Collimator2Crystal

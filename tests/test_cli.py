@@ -102,3 +102,55 @@ def test_scattergen_surrogate_flag(tmp_path):
         assert np.median(err) <= 0.01 and err.max() <= 0.05, (np.median(err), err.max())
     r = run("ScatterGen_CircularHole", ["-surrogate", "0"], tmp_path)
     assert r.returncode != 0
+
+
+@pytest.mark.gpu
+def test_bitmap_files_carry_a_geometry_hash(tmp_path):
+    """Bitmap files come with "<file>.geohash"; a -Geo* file whose hash names
+    another geometry is recomputed (the reference would reuse it); a file with
+    no .geohash is read as the reference reads it."""
+    p = configs.tiny(seed=4, rotated=True)
+    p.write_dat(str(tmp_path))
+    assert run("PEGen_CircularHole", [], tmp_path).returncode == 0
+    r = run("ScatterGen_CircularHole", [], tmp_path)
+    assert r.returncode == 0, r.stderr
+    ctx = sysmat_b200.Context(0)
+    g = sysmat_b200.Geometry(ctx, p)
+    hc, hh = g.bitmap_hashes()
+    g.close()
+    for name, h, kind in (("GeometryRelationShip_Crystal2Crystal", hc, "crystal"),
+                          ("GeometryRelationShip_Collimator2Crystal", hh, "collimator")):
+        text = (tmp_path / (name + ".geohash")).read_text()
+        assert text.startswith("sysmat_b200-bitmap-v1 %s " % kind) and ("fnv1a64=%016x" % h) in text
+    for a, b in (("GeometryRelationShip_Crystal2Crystal", "gc"), ("GeometryRelationShip_Collimator2Crystal", "gh")):
+        os.rename(tmp_path / a, tmp_path / b)
+        os.rename(tmp_path / (a + ".geohash"), tmp_path / (b + ".geohash"))
+    r = run("ScatterGen_CircularHole", ["-GeoCrystal", "gc", "-GeoCollimator", "gh"], tmp_path)
+    assert r.returncode == 0 and "another geometry" not in r.stderr
+    # move one crystal: the PE sysmat and both bitmaps change
+    q = p.copy()
+    q.detector = q.detector.copy()
+    q.detector[1 + 12 * 3] += 0.7
+    q.write_dat(str(tmp_path))
+    assert run("PEGen_CircularHole", [], tmp_path).returncode == 0
+    stale_c, stale_h = (tmp_path / "gc").read_bytes(), (tmp_path / "gh").read_bytes()
+    r = run("ScatterGen_CircularHole", ["-GeoCrystal", "gc", "-GeoCollimator", "gh"], tmp_path)
+    assert r.returncode == 0, r.stderr
+    assert r.stderr.count("computed for another geometry") == 2 * 2    # two rotations, two files
+    N, V = q.n_crystals, q.n_voxels
+    pe = np.fromfile(tmp_path / shift_name("PE_SysMat", q), np.float32).reshape(2, N, V)
+    sc = np.fromfile(tmp_path / shift_name("Scatter_SysMat", q), np.float32).reshape(2, N, V)
+    g = sysmat_b200.Geometry(ctx, q)
+    for rot in range(2):
+        assert np.array_equal(sc[rot], g.scatter(pe=pe[rot], rotation=rot))
+    fresh_c, fresh_h = g.scatter_bitmaps()
+    g.close()
+    assert (tmp_path / "gc").read_bytes() == fresh_c.tobytes() != stale_c
+    assert (tmp_path / "gh").read_bytes() == fresh_h.tobytes()
+    # without .geohash a file is taken as it is (the reference's behaviour)
+    (tmp_path / "gc").write_bytes(stale_c)
+    os.remove(tmp_path / "gc.geohash")
+    r = run("ScatterGen_CircularHole", ["-GeoCrystal", "gc", "-GeoCollimator", "gh"], tmp_path)
+    assert r.returncode == 0 and "another geometry" not in r.stderr
+    assert (tmp_path / "gc").read_bytes() == stale_c
+    ctx.close()
