@@ -136,7 +136,8 @@ def test_bitmap_files_carry_a_geometry_hash(tmp_path):
     stale_c, stale_h = (tmp_path / "gc").read_bytes(), (tmp_path / "gh").read_bytes()
     r = run("ScatterGen_CircularHole", ["-GeoCrystal", "gc", "-GeoCollimator", "gh"], tmp_path)
     assert r.returncode == 0, r.stderr
-    assert r.stderr.count("computed for another geometry") == 2 * 2    # two rotations, two files
+    # once per file: the first rotation refreshes both files, the second reads them
+    assert r.stderr.count("computed for another geometry") == 2
     N, V = q.n_crystals, q.n_voxels
     pe = np.fromfile(tmp_path / shift_name("PE_SysMat", q), np.float32).reshape(2, N, V)
     sc = np.fromfile(tmp_path / shift_name("Scatter_SysMat", q), np.float32).reshape(2, N, V)
