@@ -437,6 +437,7 @@ def run_ours(args, world, rank, local):
             line["scatter"] = run_scatter(args, ctx, dev)
         if world == 1 and args.sweep_steps > 0:
             line["sweep"] = run_sweep(args, ctx, dev)
+            line["rotations"] = run_rotations(args, ctx, dev)
         if world == 1 and args.surrogate_steps > 0:
             line["surrogate"] = run_surrogate(args, ctx, dev)
         print(json.dumps(line))
@@ -688,6 +689,65 @@ def run_sweep(args, ctx, dev):
             "bricks": sorted(set(tuple(o.tile_voxels) for o in opts)),
             "timed": "one CUDA-graph launch of the persistent kernel vs 64 sm_pe_compute launches on one stream, "
                      "same autotuned bricks, CUDA events, best of %d" % args.sweep_steps}
+
+
+# ---------------------------------------------------------------------------
+# Rotations as work items of one persistent launch (the CLI's multi-rotation path)
+# ---------------------------------------------------------------------------
+
+def run_rotations(args, ctx, dev, n_rot: int = 16):
+    """pe_small's geometry turned through n_rot image rotations (2 pi / n_rot
+    apart), voxel centres x 2x4x2 sub-cells: every rotation's whole matrix in
+    one persistent launch (sm_pe_batch with per-item rotations, CUDA graph) vs
+    one sm_pe_compute launch per rotation, outputs resident in HBM."""
+    import torch
+    import sysmat_b200
+    from sysmat_b200 import configs
+    p = configs.pe_small()
+    p.image = p.image.copy()
+    p.image[6] = n_rot
+    p.image[7] = np.float32(2 * np.pi / n_rot)
+    p.sv = (1, 1, 1)
+    g = sysmat_b200.Geometry(ctx, p)
+    opts = g.options()
+    N, V = p.n_crystals, p.n_voxels
+    outs = torch.empty((n_rot, N, V), dtype=torch.float32, device=dev)
+    stream = torch.cuda.Stream(device=dev)
+    batch = sysmat_b200.PeBatch(ctx, [g] * n_rot, [opts] * n_rot, [outs[r].data_ptr() for r in range(n_rot)],
+                                [V] * n_rot, rotations=list(range(n_rot)))
+
+    def timed(fn, reps=3):
+        best = 1e30
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            with torch.cuda.stream(stream):
+                e0.record(stream)
+                fn()
+                e1.record(stream)
+            stream.synchronize()
+            best = min(best, e0.elapsed_time(e1) / 1e3)
+        return best
+
+    batch.run(stream.cuda_stream)
+    stream.synchronize()
+    t_batch = timed(lambda: batch.run(stream.cuda_stream))
+    ref = outs.clone()
+
+    def per_rotation():
+        for r in range(n_rot):
+            g.pe(rotation=r, opts=opts, out=outs[r].data_ptr(), stream=stream.cuda_stream)
+    t_seq = timed(per_rotation)
+    ctx.sync(stream.cuda_stream)
+    same = bool(torch.equal(ref, outs))
+    batch.close()
+    g.close()
+    entries = n_rot * N * V
+    return {"workload": "pe_small geometry, %d image rotations, voxel centres x 2x4x2 sub-cells [%d x %d] per rotation"
+                        % (n_rot, N, V),
+            "batched_s": t_batch, "per_rotation_s": t_seq, "speedup": t_seq / t_batch,
+            "batched_entries_per_s": entries / t_batch, "identical_outputs": same,
+            "timed": "one CUDA-graph launch of the persistent kernel over %d rotations vs %d sm_pe_compute launches, "
+                     "CUDA events, best of 3" % (n_rot, n_rot)}
 
 
 def main():

@@ -7,11 +7,15 @@
 // directory and writes PE_SysMat_shift_<x>_<y>_<z>.sysmat: float32
 // [rotation][crystal][voxel x + nx (y + ny z)].  Defaults reproduce the
 // reference (voxel centre, 8 x 16 x 8 crystal sub-cells); -sv / -sc set voxel
-// sub-samples and crystal sub-cells.  Slabs of z-planes are computed on the
-// device while the previous slab is written to the file.
+// sub-samples and crystal sub-cells.  Several rotations run as the work items
+// of one persistent launch (the reference launches once per slab and
+// rotation, PEGen_CircularHole.cpp:167-223); a matrix too large for that goes
+// by slabs of z-planes.  The file is written while the device computes.
 #include <algorithm>
 #include <cstring>
 #include <thread>
+
+#include <cuda_runtime.h>
 
 #include "cli_common.h"
 #include "sysmat_b200.h"
@@ -65,38 +69,99 @@ int main(int argc, char* argv[]) {
         std::fprintf(stderr, "ERROR: open sysmat output %s\n", name.c_str());
         return 1;
     }
-    // slabs of whole z-planes, at most 1 GiB of host buffer each, two buffers
-    const int64_t plane = (int64_t)g.nx * g.ny;
-    int slab = (int)std::max<int64_t>(1, ((int64_t)1 << 28) / std::max<int64_t>(1, (int64_t)g.n_crystals * plane));
-    slab = std::min(slab, g.nz);
-    std::vector<float> buf[2];
-    buf[0].resize((size_t)g.n_crystals * plane * slab);
-    buf[1].resize(buf[0].size());
     std::thread writer;
     bool write_ok = true;
-    int which = 0;
-    for (int rot = 0; rot < g.n_rotations; ++rot) {
-        std::printf("########################\nRotation (%d) processing ...\n########################\n", rot);
-        for (int z0 = 0; z0 < g.nz; z0 += slab) {
-            const int nz = std::min(slab, g.nz - z0);
-            const int64_t cols = plane * nz;
-            float* out = buf[which].data();
-            if (sm_pe_compute(ctx, geo, &opt, rot, 0, g.n_crystals, z0, nz, out, cols, 0, nullptr) != SM_OK) {
+    const int64_t plane = (int64_t)g.nx * g.ny;
+    const int64_t rot_floats = (int64_t)g.n_crystals * g.voxels;
+    // Whole rotations as the work items of one persistent launch (sm_pe_batch)
+    // when a rotation's matrix fits the device budget: up to 64 rotations per
+    // launch, at most 4 GiB of output per group, written while the next group
+    // computes.  Otherwise slabs of z-planes, one sm_pe_compute per slab.
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) free_b = 0;
+    const int64_t budget = std::min<int64_t>((int64_t)4 << 30, (int64_t)(free_b / 4));
+    const int group = (int)std::min<int64_t>({(int64_t)g.n_rotations, 64, budget / std::max<int64_t>(1, 4 * rot_floats)});
+    if (group >= 1 && g.n_rotations > 1) {
+        float* d_out = nullptr;
+        if (cudaMalloc(&d_out, sizeof(float) * (size_t)rot_floats * (size_t)group) != cudaSuccess) {
+            std::fprintf(stderr, "ERROR: device allocation of %d rotations failed\n", group);
+            return 1;
+        }
+        std::vector<float> host[2];
+        int which = 0;
+        for (int r0 = 0; r0 < g.n_rotations; r0 += group) {
+            const int nr = std::min(group, g.n_rotations - r0);
+            std::vector<const sm_geometry*> geos(nr, geo);
+            std::vector<sm_pe_options> opts(nr, opt);
+            std::vector<int> rots(nr);
+            std::vector<float*> dst(nr);
+            std::vector<int64_t> lds(nr, g.voxels);
+            for (int i = 0; i < nr; ++i) {
+                rots[i] = r0 + i;
+                dst[i] = d_out + (size_t)i * (size_t)rot_floats;
+            }
+            std::printf("########################\nRotations (%d..%d) processing in one launch ...\n"
+                        "########################\n", r0, r0 + nr - 1);
+            sm_pe_batch* batch = nullptr;
+            int rc = sm_pe_batch_create(ctx, nr, geos.data(), opts.data(), rots.data(), dst.data(), lds.data(), &batch);
+            if (rc == SM_OK) rc = sm_pe_batch_run(batch, nullptr);
+            if (rc == SM_OK) rc = sm_context_sync(ctx, nullptr);
+            sm_pe_batch_destroy(batch);
+            if (rc != SM_OK) {
                 std::fprintf(stderr, "ERROR: %s\n", sm_last_error());
                 if (writer.joinable()) writer.join();
                 return 3;
             }
             if (writer.joinable()) writer.join();
-            // rows of this slab go to [rot][det][z0 * plane ...] (PEGen_CircularHole.cpp:202-216)
+            host[which].resize((size_t)rot_floats * (size_t)nr);
+            if (cudaMemcpy(host[which].data(), d_out, sizeof(float) * host[which].size(), cudaMemcpyDeviceToHost) !=
+                cudaSuccess) {
+                std::fprintf(stderr, "ERROR: copying rotations %d..%d to the host failed\n", r0, r0 + nr - 1);
+                return 3;
+            }
+            // rotations r0 .. r0 + nr - 1 are contiguous in the file ([rotation][crystal][voxel])
+            const float* src = host[which].data();
+            const size_t n = host[which].size();
             writer = std::thread([=, &write_ok] {
-                for (int d = 0; d < g.n_crystals; ++d) {
-                    const int64_t off = (((int64_t)rot * g.n_crystals + d) * g.voxels + (int64_t)z0 * plane) * 4;
-                    if (fseeko(fp, (off_t)off, SEEK_SET) != 0 || !cli::write_all(fp, out + (int64_t)d * cols, (size_t)cols))
-                        write_ok = false;
-                }
+                if (fseeko(fp, (off_t)((int64_t)r0 * rot_floats * 4), SEEK_SET) != 0 || !cli::write_all(fp, src, n))
+                    write_ok = false;
             });
-            std::printf("WROTE slab z0=%d slabZ=%d bins=%lld\n", z0, nz, (long long)cols);
             which ^= 1;
+        }
+        if (writer.joinable()) writer.join();
+        cudaFree(d_out);
+    } else {
+        // slabs of whole z-planes, at most 1 GiB of host buffer each, two buffers
+        int slab = (int)std::max<int64_t>(1, ((int64_t)1 << 28) / std::max<int64_t>(1, (int64_t)g.n_crystals * plane));
+        slab = std::min(slab, g.nz);
+        std::vector<float> buf[2];
+        buf[0].resize((size_t)g.n_crystals * plane * slab);
+        buf[1].resize(buf[0].size());
+        int which = 0;
+        for (int rot = 0; rot < g.n_rotations; ++rot) {
+            std::printf("########################\nRotation (%d) processing ...\n########################\n", rot);
+            for (int z0 = 0; z0 < g.nz; z0 += slab) {
+                const int nz = std::min(slab, g.nz - z0);
+                const int64_t cols = plane * nz;
+                float* out = buf[which].data();
+                if (sm_pe_compute(ctx, geo, &opt, rot, 0, g.n_crystals, z0, nz, out, cols, 0, nullptr) != SM_OK) {
+                    std::fprintf(stderr, "ERROR: %s\n", sm_last_error());
+                    if (writer.joinable()) writer.join();
+                    return 3;
+                }
+                if (writer.joinable()) writer.join();
+                // rows of this slab go to [rot][det][z0 * plane ...] (PEGen_CircularHole.cpp:202-216)
+                writer = std::thread([=, &write_ok] {
+                    for (int d = 0; d < g.n_crystals; ++d) {
+                        const int64_t off = (((int64_t)rot * g.n_crystals + d) * g.voxels + (int64_t)z0 * plane) * 4;
+                        if (fseeko(fp, (off_t)off, SEEK_SET) != 0 ||
+                            !cli::write_all(fp, out + (int64_t)d * cols, (size_t)cols))
+                            write_ok = false;
+                    }
+                });
+                std::printf("WROTE slab z0=%d slabZ=%d bins=%lld\n", z0, nz, (long long)cols);
+                which ^= 1;
+            }
         }
     }
     if (writer.joinable()) writer.join();

@@ -155,3 +155,27 @@ def test_bitmap_files_carry_a_geometry_hash(tmp_path):
     assert r.returncode == 0 and "another geometry" not in r.stderr
     assert (tmp_path / "gc").read_bytes() == stale_c
     ctx.close()
+
+
+@pytest.mark.gpu
+def test_pegen_rotations_as_items_of_one_launch(tmp_path):
+    """Several rotations go through one persistent launch (sm_pe_batch with
+    per-item rotations); the file equals sm_pe_compute per rotation."""
+    p = configs.tiny(seed=2, rotated=True)
+    p.image = p.image.copy()
+    p.image[6] = 5
+    p.image[7] = 0.2
+    p.write_dat(str(tmp_path))
+    r = run("PEGen_CircularHole", ["-sv", "2", "1", "2", "-sc", "2", "4", "2"], tmp_path)
+    assert r.returncode == 0, r.stderr
+    assert "Rotations (0..4) processing in one launch" in r.stdout
+    N, V = p.n_crystals, p.n_voxels
+    pe = np.fromfile(tmp_path / shift_name("PE_SysMat", p), np.float32).reshape(5, N, V)
+    ctx = sysmat_b200.Context(0)
+    g = sysmat_b200.Geometry(ctx, p)
+    opts = sysmat_b200.PeOptions.make((2, 1, 2), (2, 4, 2))
+    for rot in range(5):
+        assert np.array_equal(pe[rot], g.pe(rotation=rot, opts=opts)), rot
+    assert len({pe[r].tobytes() for r in range(5)}) == 5
+    g.close()
+    ctx.close()
