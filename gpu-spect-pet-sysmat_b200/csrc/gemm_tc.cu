@@ -17,8 +17,12 @@
 // buffer is refilled.  The epilogue reads TMEM (warp w owns rows 32w..32w+31)
 // and writes each thread's row segment as whole 32-byte sectors.
 //
-// Every wait is bounded: a wait that runs out sets the error word and the
-// CTA skips its epilogue, frees its TMEM and returns.
+// Every wait is bounded (wait_limit polls, set process-wide by
+// sm_tc_wait_limit): a wait that runs out sets the error word and the CTA
+// skips its epilogue; threads whose wait ran out then wait (bounded by the
+// default limit) for their MMAs still in flight, and the CTA frees its TMEM
+// and returns.
+#include <atomic>
 #include <cstdint>
 
 #include <cuda_bf16.h>
@@ -65,7 +69,7 @@ __device__ __forceinline__ void stage(__nv_bfloat16* dst, int n_rows, const __nv
     }
 }
 
-__global__ void __launch_bounds__(kGemmThreads) gemm_bf16_tc_kernel(GemmArgs g) {
+__global__ void __launch_bounds__(kGemmThreads) gemm_bf16_tc_kernel(GemmArgs g, uint32_t wait_limit) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     GemmSmem& S = *reinterpret_cast<GemmSmem*>(smem_raw);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -85,6 +89,7 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_bf16_tc_kernel(GemmArgs g) 
 
     uint32_t phase = 0;
     bool ok = true;
+    bool pending = false;   // this thread's wait ran out with MMAs possibly still in flight
     const int n_chunks = (g.k + kChunkK - 1) / kChunkK;
     for (int c = 0; c < n_chunks && ok; ++c) {
         const int k0 = c * kChunkK;
@@ -95,9 +100,10 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_bf16_tc_kernel(GemmArgs g) 
         __syncthreads();
         if (threadIdx.x == 0) mma_chunk(tmem, S.a, S.b, idesc, c == 0, &S.mbar);
         // the MMAs must finish reading the buffers before they are refilled
-        if (!mbar_wait(&S.mbar, phase)) {
+        if (!mbar_wait(&S.mbar, phase, wait_limit)) {
             S.failed = 1;
             ok = false;
+            pending = true;
         } else {
             phase ^= 1u;
         }
@@ -132,8 +138,8 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_bf16_tc_kernel(GemmArgs g) 
             }
         }
     } else {
-        // give MMAs still in flight one more bounded wait before the TMEM is released
-        mbar_wait(&S.mbar, phase);
+        // MMAs still in flight get one more bounded wait before the TMEM is released
+        if (pending) mbar_wait(&S.mbar, phase, kWaitLimit);
         if (threadIdx.x == 0 && g.error) atomicOr(g.error, 1);
     }
     asm volatile("tcgen05.fence::before_thread_sync;");
@@ -141,7 +147,16 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_bf16_tc_kernel(GemmArgs g) 
     if (warp == 0) tmem_dealloc(tmem, (uint32_t)g.n_tile);
 }
 
+std::atomic<uint32_t> g_wait_limit{kWaitLimit};
+
 }  // namespace
+
+uint32_t gemm_wait_limit(int64_t polls) {
+    const uint32_t prev = g_wait_limit.load();
+    if (polls < 0) g_wait_limit.store(kWaitLimit);
+    else g_wait_limit.store(polls > 0xffffffffLL ? 0xffffffffu : (uint32_t)polls);
+    return prev;
+}
 
 cudaError_t gemm_bf16_tc(const GemmArgs& args, cudaStream_t stream) {
     if (args.m <= 0 || args.n <= 0 || args.k <= 0) return cudaSuccess;
@@ -156,7 +171,7 @@ cudaError_t gemm_bf16_tc(const GemmArgs& args, cudaStream_t stream) {
         if (dev < 64) done |= 1ULL << dev;
     }
     dim3 grid((args.m + kTileM - 1) / kTileM, (args.n + args.n_tile - 1) / args.n_tile);
-    gemm_bf16_tc_kernel<<<grid, kGemmThreads, sizeof(GemmSmem), stream>>>(args);
+    gemm_bf16_tc_kernel<<<grid, kGemmThreads, sizeof(GemmSmem), stream>>>(args, g_wait_limit.load());
     return cudaGetLastError();
 }
 

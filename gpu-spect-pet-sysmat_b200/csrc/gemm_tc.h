@@ -30,4 +30,8 @@ struct GemmArgs {
 
 cudaError_t gemm_bf16_tc(const GemmArgs& args, cudaStream_t stream);
 
+// Sets the mbarrier poll limit of later gemm_bf16_tc launches (polls < 0: the
+// default); returns the previous limit.
+uint32_t gemm_wait_limit(int64_t polls);
+
 }  // namespace smb

@@ -33,3 +33,9 @@ extern "C" int sm_gemm_bf16(int m, int n, int k, const void* a, int64_t a_ms, in
     SM_CUDA(gemm_bf16_tc(g, (cudaStream_t)stream));
     return SM_OK;
 }
+
+extern "C" int sm_tc_wait_limit(int64_t polls, int64_t* previous) {
+    const uint32_t prev = gemm_wait_limit(polls);
+    if (previous) *previous = (int64_t)prev;
+    return SM_OK;
+}

@@ -49,9 +49,10 @@ __device__ __forceinline__ void mbar_init(unsigned long long* bar, uint32_t coun
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
 }
 
-__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, uint32_t phase) {
+// Polls until the phase completes or `limit` polls have failed (false).
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, uint32_t phase, uint32_t limit = kWaitLimit) {
     const uint32_t a = smem_u32(bar);
-    for (uint32_t it = 0; it < kWaitLimit; ++it) {
+    for (uint32_t it = 0; it < limit; ++it) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"

@@ -160,6 +160,7 @@ PROTOTYPES = {
                                          _i32p, ctypes.c_int, _i32p, ctypes.c_int, _vp, ctypes.c_int64, _vp]),
     "sm_scatter_transfer": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(ScatterOptions), ctypes.c_int, _vp, ctypes.c_int,
                                            _vp, ctypes.c_int64, _vp]),
+    "sm_tc_wait_limit": (ctypes.c_int, [ctypes.c_int64, _i64p]),
     "sm_surrogate_options_default": (None, [ctypes.POINTER(SurrogateOptions)]),
     "sm_scatter_surrogate": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(SurrogateOptions), ctypes.c_int, _vp,
                                             ctypes.c_int64, _vp, ctypes.c_int64, _f32p, _i32p,
@@ -552,6 +553,14 @@ def gemm_bf16(m: int, n: int, k: int, a: int, a_strides, b: int, b_strides, c: i
                               int(b_strides[0]), int(b_strides[1]), _vp(c), int(ldc), float(alpha),
                               _vp(row_scale) if row_scale else None, _vp(bias) if bias else None, 1 if accumulate else 0,
                               int(n_tile), _vp(error) if error else None, _vp(stream)))
+
+
+def tc_wait_limit(polls: int) -> int:
+    """sm_tc_wait_limit: sets the tensor-core GEMMs' bounded-wait limit
+    (polls < 0 restores the default); returns the previous limit."""
+    prev = ctypes.c_int64(0)
+    _check(lib().sm_tc_wait_limit(int(polls), ctypes.byref(prev)))
+    return int(prev.value)
 
 
 class SurrogateNet:

@@ -291,6 +291,15 @@ int sm_gemm_bf16(int m, int n, int k, const void* a, int64_t a_ms, int64_t a_ks,
                  int64_t b_ks, float* c, int64_t ldc, float alpha, const float* row_scale, const float* bias,
                  int accumulate, int n_tile, int* error, void* stream);
 
+/* The bound on every wait of sm_gemm_bf16 (and of the surrogate network's
+ * GEMMs) for its own MMAs: mbarrier polls before the kernel gives up, sets
+ * *error, skips its epilogue, waits (bounded by the default) for MMAs still in
+ * flight, frees its tensor memory and returns.  Process-wide; applies to
+ * launches after the call.  polls < 0 restores the default (2^26); 0 makes
+ * every wait give up at once (for testing the error path).  previous (may be
+ * NULL) receives the limit in force before. */
+int sm_tc_wait_limit(int64_t polls, int64_t* previous);
+
 /* ---- scatter surrogate ------------------------------------------------------------ */
 /* No reference counterpart.  The crystal-scatter sysmat from a physics
  * baseline plus a learned correction, verified against the exact kernels:

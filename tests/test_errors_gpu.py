@@ -69,3 +69,34 @@ def test_candidate_overflow_is_capacity_error_static_entry():
     with pytest.raises(sysmat_b200.SysmatError) as e:
         sysmat_b200.pe_compute_static(p, dst.data_ptr(), p.n_voxels)
     assert e.value.code == -2 and "candidate" in str(e.value)
+
+
+def test_gemm_wait_running_out_is_reported_skips_epilogue_and_frees_tensor_memory():
+    """With a wait limit of 0 polls every bounded wait of the tensor-core GEMM
+    gives up at once: the kernel sets the error word, writes nothing, waits for
+    its own MMAs and frees its tensor memory; a GEMM launched afterwards with
+    the default limit allocates tensor memory again and is correct."""
+    import torch
+    torch.manual_seed(5)
+    m, n, k = 256, 256, 192
+    a = torch.randn(m, k, device="cuda").bfloat16()
+    b = torch.randn(n, k, device="cuda").bfloat16()
+    c = torch.full((m, n), float("nan"), device="cuda")
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    prev = sysmat_b200.tc_wait_limit(0)
+    try:
+        sysmat_b200.gemm_bf16(m, n, k, a.data_ptr(), (k, 1), b.data_ptr(), (k, 1), c.data_ptr(), n, n_tile=256,
+                              error=err.data_ptr())
+        torch.cuda.synchronize()
+    finally:
+        assert sysmat_b200.tc_wait_limit(-1) == 0
+    assert prev == 1 << 26
+    assert int(err.item()) == 1
+    assert torch.isnan(c).all()            # epilogue skipped
+    err.zero_()
+    sysmat_b200.gemm_bf16(m, n, k, a.data_ptr(), (k, 1), b.data_ptr(), (k, 1), c.data_ptr(), n, n_tile=256,
+                          error=err.data_ptr())
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    ref = a.float() @ b.float().T
+    assert ((c - ref).abs() / ref.abs().amax(1, keepdim=True)).max().item() <= 1e-4
