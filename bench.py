@@ -437,6 +437,7 @@ def run_ours(args, world, rank, local):
             line["scatter"] = run_scatter(args, ctx, dev)
         if world == 1 and args.sweep_steps > 0:
             line["sweep"] = run_sweep(args, ctx, dev)
+            line["sweep_small"] = run_sweep(args, ctx, dev, small=True)
             line["rotations"] = run_rotations(args, ctx, dev)
         if world == 1 and args.surrogate_steps > 0:
             line["surrogate"] = run_surrogate(args, ctx, dev)
@@ -634,11 +635,11 @@ def run_surrogate(args, ctx, dev):
 # Batched design sweep: 64 seeded geometries in one persistent graph launch
 # ---------------------------------------------------------------------------
 
-def run_sweep(args, ctx, dev):
+def run_sweep(args, ctx, dev, small: bool = False):
     import torch
     import sysmat_b200
     from sysmat_b200 import configs
-    params = configs.sweep()
+    params = configs.sweep_small() if small else configs.sweep()
     geos = [sysmat_b200.Geometry(ctx, p) for p in params]
     t0 = time.perf_counter()
     opts = []
@@ -679,14 +680,16 @@ def run_sweep(args, ctx, dev):
     batch.close()
     for g in geos:
         g.close()
-    return {"workload": "64 seeded geometries (grids 16^3..48^3, 1-3 plates, 16-400 holes per plate, 16^2..48^2 "
-                        "crystals x 1-4 layers), whole PE sysmat of each, voxel centres x 2x4x2 sub-cells",
+    workload = ("64 small seeded geometries (grids 8^3..20^3, 1-2 plates of 16-100 holes, 8^2..24^2 crystals x 1-2 "
+                "layers)" if small else "64 seeded geometries (grids 16^3..48^3, 1-3 plates, 16-400 holes per plate, "
+                                        "16^2..48^2 crystals x 1-4 layers)")
+    return {"workload": workload + ", whole PE sysmat of each, voxel centres x 2x4x2 sub-cells",
             "entries": entries, "rays": rays, "output_gb": entries * 4 / 1e9,
             "batched_s": t_batch, "batched_entries_per_s": entries / t_batch, "batched_rays_per_s": rays / t_batch,
             "sequential_s": t_seq, "sequential_entries_per_s": entries / t_seq, "speedup": t_seq / t_batch,
             "sequential_default_brick_s": t_default, "autotune_gain": t_default / t_seq,
             "work_items": info["items"], "persistent_ctas": info["ctas"], "autotune_s": tune_s,
-            "bricks": sorted(set(tuple(o.tile_voxels) for o in opts)),
+            "bricks": sorted(set(tuple(o.tile_voxels) + (o.group,) for o in opts)),
             "timed": "one CUDA-graph launch of the persistent kernel vs 64 sm_pe_compute launches on one stream, "
                      "same autotuned bricks, CUDA events, best of %d" % args.sweep_steps}
 

@@ -73,6 +73,8 @@ int validate_pe(const sm_geometry* geo, const sm_pe_options* opt, int row0, int 
     }
     if ((int64_t)opt->sv[0] * opt->sv[1] * opt->sv[2] * opt->sc[0] * opt->sc[1] * opt->sc[2] > (1 << 22))
         return fail(SM_ERR_CAPACITY, "more than 2^22 rays per entry");
+    if (opt->group < 0 || opt->group > kMaxGroup)
+        return fail(SM_ERR_INVALID, "group = %d must be 0 (auto) or 1..%d", opt->group, kMaxGroup);
     const HostGeometry& g = geo->host;
     if ((int64_t)g.nx * opt->sv[0] > (1 << 24) || (int64_t)g.ny * opt->sv[1] > (1 << 24) ||
         (int64_t)g.nz * opt->sv[2] > (1 << 24))
@@ -251,7 +253,7 @@ int sm_pe_compute(sm_context* ctx, const sm_geometry* geo, const sm_pe_options* 
     sm_pe_options tuned = *opt;
     if (opt->flags & SM_PE_AUTOTUNE) SM_TRY(sm_pe_autotune(ctx, geo, opt, rotation, &tuned, nullptr));
     PEParams P;
-    pe_plan(g, tuned.sv, tuned.sc, tuned.tile_voxels, rotation, row0, row1, g.nz, z0, nz, &P);
+    pe_plan(g, tuned.sv, tuned.sc, tuned.tile_voxels, tuned.group, rotation, row0, row1, g.nz, z0, nz, &P);
     P.status = ctx->d_status;
     P.counters = ctx->collect_counters ? ctx->d_counters : nullptr;
     if (P.counters) SM_CUDA(cudaMemsetAsync(ctx->d_counters, 0, 4 * sizeof(unsigned long long), stream));
@@ -298,7 +300,7 @@ int sm_pe_record_hits(sm_context* ctx, const sm_geometry* geo, const sm_pe_optio
     SM_TRY(validate_pe(geo, opt, 0, geo->host.n_crystals, 0, geo->host.nz));
     const HostGeometry& g = geo->host;
     PEParams P;
-    pe_plan(g, opt->sv, opt->sc, opt->tile_voxels, rotation, 0, g.n_crystals, g.nz, 0, g.nz, &P);
+    pe_plan(g, opt->sv, opt->sc, opt->tile_voxels, opt->group, rotation, 0, g.n_crystals, g.nz, 0, g.nz, &P);
     const int64_t vox_n = (int64_t)g.nx * g.ny * g.nz;
     std::vector<long long> tiles;
     for (int64_t i = 0; i < n; ++i) {
@@ -375,7 +377,7 @@ int PESysMatGen(float* parameter_Collimator, float* parameter_Detector, float* p
     sm_pe_options_reference(&opt);
     PEParams P;
     const int64_t slab = (int64_t)g.nx * g.ny * nz_slab;
-    pe_plan(g, opt.sv, opt.sc, opt.tile_voxels, rotation_index, 0, g.n_crystals, nz_full, z0, nz_slab, &P);
+    pe_plan(g, opt.sv, opt.sc, opt.tile_voxels, opt.group, rotation_index, 0, g.n_crystals, nz_full, z0, nz_slab, &P);
     // The kernel indexes slab-local columns from z0; a legacy slab is "z0..z0+nz of
     // a volume of nz_full planes", so the slab's own z range is [z0, z0 + nz_slab).
     float angle = parameter_Image[20] * parameter_Image[7];

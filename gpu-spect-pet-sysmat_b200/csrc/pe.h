@@ -61,8 +61,13 @@ struct PEParams {
 
 // Fills every field of `p` but the output, status and record pointers, for the
 // slab [z0, z0 + nz) of a volume of nz_full z-planes and rows [row0, row1).
-void pe_plan(const HostGeometry& g, const int sv[3], const int sc[3], const int brick[3], int rotation,
+// group: voxel sub-points per warp pass (0 = auto, the fewest that fill the
+// 32 lanes, at most kMaxGroup).  Every lane traces rays (sub-point, sub-cell)
+// Q = lane, lane + 32, ... in the same order for every group with
+// group * sub-cells a multiple of 32, so those groups give identical results.
+void pe_plan(const HostGeometry& g, const int sv[3], const int sc[3], const int brick[3], int group, int rotation,
              int row0, int row1, int nz_full, int z0, int nz, PEParams* p);
+int pe_auto_group(int n_subcells);
 
 // Launches the trace kernel (RECORD selects the hit-recording instantiation).
 cudaError_t pe_launch(const PEParams& p, const DevGeometry& geo, bool record, long long n_tiles, cudaStream_t stream);

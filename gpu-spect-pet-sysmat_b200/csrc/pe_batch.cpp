@@ -4,9 +4,10 @@
 // The persistent kernel (pe_kernel.cu, pe_batch_kernel) hands out (geometry,
 // tile) items from one counter; geometries are ordered by estimated cost,
 // largest first, so the dynamic hand-out fills the tail with small items.
-// The autotuner times candidate voxel bricks on a sample of tiles of a
-// geometry and caches the fastest per device and geometry class (in memory,
-// and in the file named by SYSMAT_B200_TUNE_CACHE when it is set).
+// The autotuner times candidate voxel bricks and sub-points per warp pass on
+// a geometry (the whole matrix when it is small, else a sample of tiles) and
+// caches the fastest per device and geometry class (in memory, and in the
+// file named by SYSMAT_B200_TUNE_CACHE when it is set).
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -45,7 +46,7 @@ namespace smb {
 namespace {
 
 std::mutex g_tune_mu;
-std::map<std::string, std::vector<int>> g_tune;   // key -> brick (x, y, z)
+std::map<std::string, std::vector<int>> g_tune;   // key -> brick (x, y, z), group
 bool g_tune_loaded = false;
 
 void tune_load_locked() {
@@ -57,17 +58,18 @@ void tune_load_locked() {
     if (!f) return;
     char key[512];
     int a, b, c;
-    while (std::fscanf(f, "%511s %d %d %d", key, &a, &b, &c) == 4) g_tune[key] = {a, b, c};
+    int gr;
+    while (std::fscanf(f, "%511s %d %d %d %d", key, &a, &b, &c, &gr) == 5) g_tune[key] = {a, b, c, gr};
     std::fclose(f);
 }
 
-void tune_store_locked(const std::string& key, const int brick[3]) {
-    g_tune[key] = {brick[0], brick[1], brick[2]};
+void tune_store_locked(const std::string& key, const int brick[3], int group) {
+    g_tune[key] = {brick[0], brick[1], brick[2], group};
     const char* path = std::getenv("SYSMAT_B200_TUNE_CACHE");
     if (!path) return;
     FILE* f = std::fopen(path, "a");
     if (!f) return;
-    std::fprintf(f, "%s %d %d %d\n", key.c_str(), brick[0], brick[1], brick[2]);
+    std::fprintf(f, "%s %d %d %d %d\n", key.c_str(), brick[0], brick[1], brick[2], group);
     std::fclose(f);
 }
 
@@ -114,17 +116,36 @@ int sm_pe_autotune(sm_context* ctx, const sm_geometry* geo, const sm_pe_options*
         auto it = g_tune.find(key);
         if (it != g_tune.end()) {
             for (int a = 0; a < 3; ++a) out->tile_voxels[a] = it->second[a];
+            out->group = it->second.size() > 3 ? it->second[3] : 0;
             if (best_ms_per_tile) *best_ms_per_tile = -1.0;
             return SM_OK;
         }
     }
-    // a block of rows and a slab of z-planes from the middle of the geometry
-    const int rows = std::min(g.n_crystals, 512);
+    // Objective: a small matrix (at most kWhole tiles with the default brick)
+    // is timed whole, tail and all, which is what its launches cost; a large
+    // one on a sample of tiles from a block of rows and a slab of z-planes in
+    // the middle of the geometry, per voxel-row processed.
+    constexpr long long kWhole = 16384;
+    PEParams P0;
+    const int zero3[3] = {0, 0, 0};
+    pe_plan(g, opt->sv, opt->sc, zero3, 0, rotation, 0, g.n_crystals, g.nz, 0, g.nz, &P0);
+    const bool whole = P0.n_tiles <= kWhole;
+    const int rows = whole ? g.n_crystals : std::min(g.n_crystals, 512);
     const int row0 = (g.n_crystals - rows) / 2;
-    const int nz = std::min(g.nz, 8);
+    const int nz = whole ? g.nz : std::min(g.nz, 8);
     const int z0 = (g.nz - nz) / 2;
     const int64_t slab = (int64_t)g.nx * g.ny * nz;
-    static const int cand[][3] = {{8, 4, 4}, {4, 4, 4}, {8, 8, 2}, {4, 4, 8}, {16, 4, 2}, {4, 8, 4}, {8, 4, 2}, {8, 8, 1}};
+    static const int cand[][3] = {{8, 4, 4}, {4, 4, 4}, {8, 8, 2}, {4, 4, 8}, {16, 4, 2}, {4, 8, 4}, {8, 4, 2}, {8, 8, 1},
+                                  {4, 4, 2}, {4, 2, 2}};
+    // sub-points per pass: the automatic value and the next that keeps every
+    // lane's ray order (group * sub-cells a multiple of 32)
+    const int n_sc = opt->sc[0] * opt->sc[1] * opt->sc[2];
+    std::vector<int> groups = {pe_auto_group(n_sc)};
+    for (int gr = groups[0] + 1; gr <= kMaxGroup; ++gr)
+        if ((gr * n_sc) % 32 == 0) {
+            groups.push_back(gr);
+            break;
+        }
     float* d_out = nullptr;
     long long* d_tiles = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -132,48 +153,54 @@ int sm_pe_autotune(sm_context* ctx, const sm_geometry* geo, const sm_pe_options*
     if (rc == SM_OK) rc = check_cuda(cudaMalloc(&d_tiles, sizeof(long long) * 4096), "autotune tiles");
     if (rc == SM_OK) rc = check_cuda(cudaEventCreate(&e0), "event");
     if (rc == SM_OK) rc = check_cuda(cudaEventCreate(&e1), "event");
-    double best = 1e300;
-    int best_brick[3] = {0, 0, 0};
+    double best = 1e300, best_ms = 0.0;
+    int best_brick[3] = {0, 0, 0}, best_group = 0;
     const int target_tiles = std::min(4096, ctx->sm_count * 2 * 4);
     for (const auto& c : cand) {
-        if (rc != SM_OK) break;
-        const int brick[3] = {c[0], c[1], c[2]};
-        PEParams P;
-        pe_plan(g, opt->sv, opt->sc, brick, rotation, row0, row0 + rows, g.nz, z0, nz, &P);
-        if (P.bx != brick[0] || P.by != brick[1] || P.bz != brick[2]) continue;   // clipped to the grid: not distinct
-        std::vector<long long> tiles;
-        const long long n = P.n_tiles;
-        const long long k = std::min<long long>(n, target_tiles);
-        for (long long i = 0; i < k; ++i) tiles.push_back(i * n / k);
-        rc = check_cuda(cudaMemcpy(d_tiles, tiles.data(), sizeof(long long) * tiles.size(), cudaMemcpyHostToDevice),
-                        "autotune tiles");
-        if (rc != SM_OK) break;
-        P.tile_list = d_tiles;
-        P.status = ctx->d_status;
-        P.dst = d_out;
-        P.ld = slab;
-        double t_best = 1e300;
-        for (int rep = 0; rep < 3 && rc == SM_OK; ++rep) {
-            rc = check_cuda(cudaEventRecord(e0, 0), "event");
-            if (rc == SM_OK) rc = check_cuda(pe_launch(P, geo->dev.view, false, (long long)tiles.size(), 0), "autotune launch");
-            if (rc == SM_OK) rc = check_cuda(cudaEventRecord(e1, 0), "event");
-            if (rc == SM_OK) rc = check_cuda(cudaEventSynchronize(e1), "autotune sync");
-            float ms = 0.0f;
-            if (rc == SM_OK) cudaEventElapsedTime(&ms, e0, e1);
-            if (rep > 0) t_best = std::min(t_best, (double)ms);   // first run warms up
-        }
-        // a brick whose sampled tiles overflow a candidate list is not a candidate
-        int st = 0;
-        if (rc == SM_OK) rc = check_cuda(cudaMemcpy(&st, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost), "status");
-        if (rc == SM_OK && st != 0) {
-            rc = check_cuda(cudaMemset(ctx->d_status, 0, sizeof(int)), "status");
-            continue;
-        }
-        // time per voxel-row processed, so candidates of different tile sizes compare
-        const double per = t_best / ((double)tiles.size() * brick[0] * brick[1] * brick[2]);
-        if (per < best) {
-            best = per;
-            std::memcpy(best_brick, brick, sizeof(best_brick));
+        for (int gr : groups) {
+            if (rc != SM_OK) break;
+            const int brick[3] = {c[0], c[1], c[2]};
+            PEParams P;
+            pe_plan(g, opt->sv, opt->sc, brick, gr, rotation, row0, row0 + rows, g.nz, z0, nz, &P);
+            if (P.bx != brick[0] || P.by != brick[1] || P.bz != brick[2]) continue;   // clipped to the grid
+            long long n_launch = P.n_tiles;
+            if (!whole) {
+                std::vector<long long> tiles;
+                const long long k = std::min<long long>(P.n_tiles, target_tiles);
+                for (long long i = 0; i < k; ++i) tiles.push_back(i * P.n_tiles / k);
+                rc = check_cuda(cudaMemcpy(d_tiles, tiles.data(), sizeof(long long) * tiles.size(),
+                                           cudaMemcpyHostToDevice), "autotune tiles");
+                if (rc != SM_OK) break;
+                P.tile_list = d_tiles;
+                n_launch = (long long)tiles.size();
+            }
+            P.status = ctx->d_status;
+            P.dst = d_out;
+            P.ld = slab;
+            double t_best = 1e300;
+            for (int rep = 0; rep < 3 && rc == SM_OK; ++rep) {
+                rc = check_cuda(cudaEventRecord(e0, 0), "event");
+                if (rc == SM_OK) rc = check_cuda(pe_launch(P, geo->dev.view, false, n_launch, 0), "autotune launch");
+                if (rc == SM_OK) rc = check_cuda(cudaEventRecord(e1, 0), "event");
+                if (rc == SM_OK) rc = check_cuda(cudaEventSynchronize(e1), "autotune sync");
+                float ms = 0.0f;
+                if (rc == SM_OK) cudaEventElapsedTime(&ms, e0, e1);
+                if (rep > 0) t_best = std::min(t_best, (double)ms);   // the first run warms up
+            }
+            // a brick whose timed tiles overflow a candidate list is not a candidate
+            int st = 0;
+            if (rc == SM_OK) rc = check_cuda(cudaMemcpy(&st, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost), "status");
+            if (rc == SM_OK && st != 0) {
+                rc = check_cuda(cudaMemset(ctx->d_status, 0, sizeof(int)), "status");
+                continue;
+            }
+            const double score = whole ? t_best : t_best / ((double)n_launch * brick[0] * brick[1] * brick[2]);
+            if (score < best) {
+                best = score;
+                best_ms = t_best / (double)n_launch;
+                std::memcpy(best_brick, brick, sizeof(best_brick));
+                best_group = gr == groups[0] ? 0 : gr;
+            }
         }
     }
     if (e0) cudaEventDestroy(e0);
@@ -184,9 +211,10 @@ int sm_pe_autotune(sm_context* ctx, const sm_geometry* geo, const sm_pe_options*
     if (rc != SM_OK) return rc;
     if (best_brick[0] == 0) return fail(SM_ERR_INVALID, "no brick candidate fits the grid");
     for (int a = 0; a < 3; ++a) out->tile_voxels[a] = best_brick[a];
-    if (best_ms_per_tile) *best_ms_per_tile = best * best_brick[0] * best_brick[1] * best_brick[2];
+    out->group = best_group;
+    if (best_ms_per_tile) *best_ms_per_tile = best_ms;
     std::lock_guard<std::mutex> lock(g_tune_mu);
-    tune_store_locked(key, best_brick);
+    tune_store_locked(key, best_brick, best_group);
     return SM_OK;
 }
 
@@ -209,7 +237,7 @@ int sm_pe_batch_create(sm_context* ctx, int n, const sm_geometry* const* geos, c
         if (!dst[i]) return fail(SM_ERR_INVALID, "geometry %d: null output", i);
         PeBatchGeom& b = items[i];
         std::memset(&b, 0, sizeof(b));
-        pe_plan(g, o.sv, o.sc, o.tile_voxels, rotations ? rotations[i] : 0, 0, g.n_crystals, g.nz, 0, g.nz, &b.P);
+        pe_plan(g, o.sv, o.sc, o.tile_voxels, o.group, rotations ? rotations[i] : 0, 0, g.n_crystals, g.nz, 0, g.nz, &b.P);
         b.P.status = ctx->d_status;
         b.P.dst = dst[i];
         b.P.ld = ld[i];

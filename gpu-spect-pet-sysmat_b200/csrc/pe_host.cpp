@@ -9,8 +9,10 @@
 
 namespace smb {
 
-void pe_plan(const HostGeometry& g, const int sv[3], const int sc[3], const int brick[3], int rotation, int row0,
-             int row1, int nz_full, int z0, int nz, PEParams* p) {
+int pe_auto_group(int n_subcells) { return std::max(1, std::min(kMaxGroup, 32 / std::max(1, n_subcells))); }
+
+void pe_plan(const HostGeometry& g, const int sv[3], const int sc[3], const int brick[3], int group, int rotation,
+             int row0, int row1, int nz_full, int z0, int nz, PEParams* p) {
     PEParams& P = *p;
     P = PEParams();
     P.nx = g.nx;
@@ -41,7 +43,7 @@ void pe_plan(const HostGeometry& g, const int sv[3], const int sc[3], const int 
     P.dZ = sc[2];
     P.n_sc = sc[0] * sc[1] * sc[2];
     P.n_sv = sv[0] * sv[1] * sv[2];
-    P.group = std::max(1, std::min(kMaxGroup, 32 / P.n_sc));
+    P.group = group > 0 ? std::min(group, kMaxGroup) : pe_auto_group(P.n_sc);
     P.inv_sv = 1.0f / (float)P.n_sv;
     P.inv_n_sc = 1.0f / (float)P.n_sc;
     P.inv_dY = 1.0f / (float)P.dY;

@@ -194,6 +194,8 @@ int validate_static(const HostGeometry& g, const sm_pe_options* opt, int row0, i
     }
     if ((int64_t)opt->sv[0] * opt->sv[1] * opt->sv[2] * opt->sc[0] * opt->sc[1] * opt->sc[2] > (1 << 22))
         return fail(SM_ERR_CAPACITY, "more than 2^22 rays per entry");
+    if (opt->group < 0 || opt->group > kMaxGroup)
+        return fail(SM_ERR_INVALID, "group = %d must be 0 (auto) or 1..%d", opt->group, kMaxGroup);
     if ((int64_t)g.nx * opt->sv[0] > (1 << 24) || (int64_t)g.ny * opt->sv[1] > (1 << 24) ||
         (int64_t)g.nz * opt->sv[2] > (1 << 24))
         return fail(SM_ERR_CAPACITY, "fine voxel grid exceeds 2^24 per axis");
@@ -258,7 +260,7 @@ extern "C" int sm_pe_compute_static(const float* collimator, size_t n_collimator
 
     cudaStream_t stream = (cudaStream_t)stream_ptr;
     PEParams P;
-    pe_plan(g, opt->sv, opt->sc, opt->tile_voxels, rotation, row0, row1, g.nz, z0, nz, &P);
+    pe_plan(g, opt->sv, opt->sc, opt->tile_voxels, opt->group, rotation, row0, row1, g.nz, z0, nz, &P);
     // The array keeps the previous call's contents: the status word must
     // start at zero, and the geometry region is overwritten in full.
     SM_CUDA(cudaMemsetAsync(base, 0, kStatusBytes, stream));

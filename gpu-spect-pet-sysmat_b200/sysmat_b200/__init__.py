@@ -39,14 +39,15 @@ class SysmatError(RuntimeError):
 
 class PeOptions(ctypes.Structure):
     _fields_ = [("sv", ctypes.c_int * 3), ("sc", ctypes.c_int * 3), ("tile_voxels", ctypes.c_int * 3),
-                ("flags", ctypes.c_int)]
+                ("flags", ctypes.c_int), ("group", ctypes.c_int)]
 
     @staticmethod
-    def make(sv=(1, 1, 1), sc=(8, 16, 8), tile_voxels=(0, 0, 0), autotune: bool = False) -> "PeOptions":
+    def make(sv=(1, 1, 1), sc=(8, 16, 8), tile_voxels=(0, 0, 0), autotune: bool = False, group: int = 0) -> "PeOptions":
         o = PeOptions()
         for i in range(3):
             o.sv[i], o.sc[i], o.tile_voxels[i] = int(sv[i]), int(sc[i]), int(tile_voxels[i])
         o.flags = 1 if autotune else 0
+        o.group = int(group)
         return o
 
 

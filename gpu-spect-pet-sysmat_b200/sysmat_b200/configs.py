@@ -17,6 +17,7 @@ Named workloads
                60/64/68/72 mm -> [6400 x 131072].  Sub-sampling as ``pe_small``.
 ``sweep``      64 seeded geometries: grids 16^3..48^3, 1-3 plates, 16-400 holes per
                plate, 16^2..48^2 crystals x 1-4 layers.
+``sweep_small`` 64 small seeded geometries (grids 8^3..20^3, 8^2..24^2 crystals).
 ``scatter_small``  32x32x16 voxels of 1 mm, the ``pe_small`` collimator, 2 layers of
                32x32 crystals (60 and 66 mm) -> [2048 x 16384].
 ``scatter_large``  the same geometry with 64x64x32 voxels -> [2048 x 131072].
@@ -113,6 +114,36 @@ def sweep(seed: int = 2, count: int = 64) -> List[Params]:
         img = build_image((n, n, n), (vox, vox, vox), fov_to_plate0=fov)
         out.append(Params(build_collimator(plates), build_detector(crystals), img, build_physics(),
                           sv=(1, 1, 1), sc=(2, 4, 2), name="sweep_%02d" % g))
+    return out
+
+
+def sweep_small(seed: int = 3, count: int = 64) -> List[Params]:
+    """``count`` small geometries (grids 8^3..20^3, 1-2 plates of 16-100 holes,
+    8^2..24^2 crystals x 1-2 layers, voxel centres): each one alone fills the
+    GPU for only a few waves of CTAs, so launch gaps and tails are a visible
+    share of per-geometry launches."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for g in range(count):
+        n = int(rng.integers(8, 21))
+        n_plates = int(rng.integers(1, 3))
+        plates = []
+        for l in range(n_plates):
+            nh_side = int(rng.integers(4, 11))
+            t = float(rng.choice([2.0, 3.0]))
+            pitch = 60.0 / nh_side
+            r = lambda: float(rng.uniform(0.3, 0.45)) * min(pitch, 2.0)  # noqa: E731
+            plates.append(_plate(80.0, t, 80.0, 6.0 * l, grid_holes(nh_side, nh_side, pitch, r, t, 6.0 * l,
+                                                                    jitter=0.15 * pitch, rng=rng)))
+        nc = int(rng.integers(8, 25))
+        n_layers = int(rng.integers(1, 3))
+        pitch = float(rng.choice([1.6, 2.0]))
+        crystals = []
+        for l in range(n_layers):
+            crystals += crystal_layer(nc, nc, pitch, (pitch, 4.0, pitch), 6.0 * (n_plates - 1) + 16.0 + 4.5 * l, CZT)
+        img = build_image((n, n, n), (1.0, 1.0, 1.0), fov_to_plate0=30.0)
+        out.append(Params(build_collimator(plates), build_detector(crystals), img, build_physics(),
+                          sv=(1, 1, 1), sc=(2, 4, 2), name="sweep_small_%02d" % g))
     return out
 
 

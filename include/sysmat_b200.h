@@ -108,7 +108,11 @@ typedef struct sm_pe_options {
     int sv[3];          /* voxel sub-samples (x, y, z); the entry is their mean  */
     int sc[3];          /* crystal sub-cells (x, y = depth, z); summed           */
     int tile_voxels[3]; /* voxel brick per CTA; 0 = default (8 x 4 x 4)          */
-    int flags;          /* SM_PE_AUTOTUNE: choose tile_voxels with sm_pe_autotune */
+    int flags;          /* SM_PE_AUTOTUNE: choose tile_voxels and group with sm_pe_autotune */
+    int group;          /* voxel sub-points a warp traces per pass, i.e. group * sc rays per
+                           pass, group * sc / 32 per lane; 0 = the fewest that fill a warp
+                           (at most 4).  Groups with group * sc[0]*sc[1]*sc[2] a multiple
+                           of 32 give identical results. */
 } sm_pe_options;
 
 enum { SM_PE_AUTOTUNE = 1 };
@@ -177,8 +181,9 @@ int sm_pe_last_counters(sm_context* ctx, int64_t out[4]);
  * replayed from a CUDA graph. */
 typedef struct sm_pe_batch sm_pe_batch;
 
-/* Times candidate voxel bricks on a sample of tiles of `geo` and writes the
- * fastest into out->tile_voxels (out = *opt otherwise).  Results are cached
+/* Times candidate voxel bricks and sub-points per pass (out->group) on `geo`
+ * (the whole matrix when it is small, else a sample of tiles) and writes the
+ * fastest into out->tile_voxels / out->group (out = *opt otherwise).  Results are cached
  * per device and geometry class for the process, and appended to the file
  * named by the environment variable SYSMAT_B200_TUNE_CACHE when it is set.
  * best_ms_per_tile (may be NULL) receives the winner's time, -1 for a cache hit. */

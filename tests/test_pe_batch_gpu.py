@@ -77,3 +77,46 @@ def test_batch_beyond_one_constant_table(ctx):
     batch.close()
     for g in geos:
         g.close()
+
+
+def _best_ms(fn, reps=5):
+    import torch
+    best = 1e30
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fn()
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    return best
+
+
+@pytest.mark.parametrize("member", [0, 7, 21])
+def test_autotuned_options_are_not_slower_and_give_the_same_matrix(ctx, member):
+    """The tuner times whole small matrices (bricks x sub-points per pass) and
+    keeps the fastest; the pick is never slower than the default options by
+    more than timing noise, and changes no value."""
+    import torch
+    p = configs.sweep_small()[member]
+    g = sysmat_b200.Geometry(ctx, p)
+    tuned, ms = sysmat_b200.autotune(g)
+    default = g.options()
+    out = torch.empty((g.n_crystals, g.nx * g.ny * g.nz), device="cuda")
+    t_default = _best_ms(lambda: g.pe(opts=default, out=out.data_ptr()))
+    t_tuned = _best_ms(lambda: g.pe(opts=tuned, out=out.data_ptr()))
+    assert t_tuned <= 1.05 * t_default + 0.01, (t_tuned, t_default, tuple(tuned.tile_voxels), tuned.group)
+    assert np.array_equal(g.pe(opts=tuned), g.pe(opts=default))
+    g.close()
+
+
+def test_group_option_keeps_values_and_is_validated(ctx):
+    p = configs.two_plates_small(seed=8)          # 16 sub-cells: groups 2 (auto) and 4 keep every lane's ray order
+    g = sysmat_b200.Geometry(ctx, p)
+    base = g.pe()
+    assert np.array_equal(g.pe(opts=sysmat_b200.PeOptions.make(p.sv, p.sc, group=4)), base)
+    assert np.array_equal(g.pe(opts=sysmat_b200.PeOptions.make(p.sv, p.sc, group=2)), base)
+    with pytest.raises(sysmat_b200.SysmatError) as e:
+        g.pe(opts=sysmat_b200.PeOptions.make(p.sv, p.sc, group=5))
+    assert e.value.code == -1 and "group" in str(e.value)
+    g.close()
