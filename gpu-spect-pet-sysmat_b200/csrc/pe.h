@@ -13,7 +13,7 @@ constexpr int kPeWarps = 8;            // warps per CTA = crystals per tile
 constexpr int kPeThreads = 32 * kPeWarps;
 constexpr int kSupC = 1024;            // tile superset capacity, crystals
 constexpr int kSupH = 384;             // tile superset capacity, holes
-constexpr int kMaxGroup = 4;           // voxel sub-points whose candidate masks are live at once
+constexpr int kMaxGroup = 8;           // voxel sub-points whose candidate masks are live at once
 constexpr int kMaxTileVoxels = 128;    // voxels per brick
 constexpr int kListC = 512;            // per-voxel candidate list capacity, crystals
 constexpr int kListH = 128;            // per-voxel candidate list capacity, holes
@@ -39,6 +39,7 @@ struct PEParams {
     float cos_a, sin_a;      // image rotation about z
     int dX, dY, dZ;          // crystal sub-cells
     int n_sc, n_sv, group;   // sub-cells per crystal, sub-points per voxel, sub-points per mask group
+    int pair;                // voxels per warp pass: 2 when a voxel has at most 16 rays, else 1
     float inv_sv;
     // reciprocals for the division-free index decode (exact after one correction step)
     float inv_n_sc, inv_dY, inv_dX, inv_kx, inv_ky, inv_kxky, inv_dXdY;
@@ -61,13 +62,15 @@ struct PEParams {
 
 // Fills every field of `p` but the output, status and record pointers, for the
 // slab [z0, z0 + nz) of a volume of nz_full z-planes and rows [row0, row1).
-// group: voxel sub-points per warp pass (0 = auto, the fewest that fill the
-// 32 lanes, at most kMaxGroup).  Every lane traces rays (sub-point, sub-cell)
-// Q = lane, lane + 32, ... in the same order for every group with
-// group * sub-cells a multiple of 32, so those groups give identical results.
+// group: voxel sub-points whose candidate masks are computed together (0 =
+// auto: 32 / depth sub-cells, so that one warp pass traces one column of
+// sub-cells from `group` sub-points, at most kMaxGroup).  Within a group the
+// rays are ordered (sub-cell column, sub-point, depth sub-cell) and dealt to
+// the lanes in order; the group changes which lane sums which ray (the
+// rounding of the sums), never a hit decision.
 void pe_plan(const HostGeometry& g, const int sv[3], const int sc[3], const int brick[3], int group, int rotation,
              int row0, int row1, int nz_full, int z0, int nz, PEParams* p);
-int pe_auto_group(int n_subcells);
+int pe_auto_group(int depth_subcells);
 
 // Launches the trace kernel (RECORD selects the hit-recording instantiation).
 cudaError_t pe_launch(const PEParams& p, const DevGeometry& geo, bool record, long long n_tiles, cudaStream_t stream);

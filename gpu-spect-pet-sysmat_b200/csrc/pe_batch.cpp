@@ -137,15 +137,10 @@ int sm_pe_autotune(sm_context* ctx, const sm_geometry* geo, const sm_pe_options*
     const int64_t slab = (int64_t)g.nx * g.ny * nz;
     static const int cand[][3] = {{8, 4, 4}, {4, 4, 4}, {8, 8, 2}, {4, 4, 8}, {16, 4, 2}, {4, 8, 4}, {8, 4, 2}, {8, 8, 1},
                                   {4, 4, 2}, {4, 2, 2}};
-    // sub-points per pass: the automatic value and the next that keeps every
-    // lane's ray order (group * sub-cells a multiple of 32)
-    const int n_sc = opt->sc[0] * opt->sc[1] * opt->sc[2];
-    std::vector<int> groups = {pe_auto_group(n_sc)};
-    for (int gr = groups[0] + 1; gr <= kMaxGroup; ++gr)
-        if ((gr * n_sc) % 32 == 0) {
-            groups.push_back(gr);
-            break;
-        }
+    // sub-points per group (rays each lane traces per group = group * sub-cells / 32):
+    // the automatic value (one column of depth sub-cells per warp pass) and half of it
+    std::vector<int> groups = {pe_auto_group(opt->sc[1])};
+    if (groups[0] >= 2) groups.push_back(groups[0] / 2);
     float* d_out = nullptr;
     long long* d_tiles = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr;

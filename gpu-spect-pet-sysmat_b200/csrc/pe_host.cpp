@@ -9,7 +9,7 @@
 
 namespace smb {
 
-int pe_auto_group(int n_subcells) { return std::max(1, std::min(kMaxGroup, 32 / std::max(1, n_subcells))); }
+int pe_auto_group(int depth_subcells) { return std::max(1, std::min(kMaxGroup, 32 / std::max(1, depth_subcells))); }
 
 void pe_plan(const HostGeometry& g, const int sv[3], const int sc[3], const int brick[3], int group, int rotation,
              int row0, int row1, int nz_full, int z0, int nz, PEParams* p) {
@@ -43,7 +43,11 @@ void pe_plan(const HostGeometry& g, const int sv[3], const int sc[3], const int 
     P.dZ = sc[2];
     P.n_sc = sc[0] * sc[1] * sc[2];
     P.n_sv = sv[0] * sv[1] * sv[2];
-    P.group = group > 0 ? std::min(group, kMaxGroup) : pe_auto_group(P.n_sc);
+    P.group = group > 0 ? std::min(group, kMaxGroup) : pe_auto_group(P.dY);
+    // An entry of at most 16 rays fills half a warp: two voxels share each
+    // warp pass, as one group of both voxels' sub-points.
+    P.pair = (P.n_sv * P.n_sc <= 16 && 2 * P.n_sv <= kMaxGroup) ? 2 : 1;
+    if (P.pair == 2) P.group = 2 * P.n_sv;
     P.inv_sv = 1.0f / (float)P.n_sv;
     P.inv_n_sc = 1.0f / (float)P.n_sc;
     P.inv_dY = 1.0f / (float)P.dY;

@@ -22,14 +22,22 @@
 //     the list (a float filter decides clear cases; cases within 1e-5 of the
 //     threshold use the reference's exact single-precision expression) and
 //     keeps the result as ballot bitmasks over the list.
-//  3. Lanes trace one ray (sub-point, sub-cell) each.  A division-free
-//     window test per candidate skips the exact test for candidates the ray
-//     cannot reach; the exact tests are the reference's single-precision
-//     ones, so every hit decision is the reference's.  Skipped candidates
-//     would have contributed exactly 0.  The plates use a fast path that
-//     proves "fully traversed" with margins, else the exact test.  Values
-//     that are not hit decisions (solid angle, path inside the detecting
-//     crystal, absorption chord) use closed forms in single precision.
+//  3. Lanes trace one ray (sub-point, sub-cell) each.  The rays of a group of
+//     sub-points are ordered (sub-cell column, sub-point, depth sub-cell) and
+//     dealt 32 to a warp pass, so a pass holds rays that run almost together
+//     through the plates and the crystals in front (one column of depth
+//     cells seen from neighbouring sub-points): the lanes meet the same
+//     candidates and take the same branches.  Each pass first narrows the
+//     candidates to those its bundle of rays can reach (window test from the
+//     voxel's sub-point box to the box of the pass's sub-cell centres).  Per
+//     ray a division-free window test skips the exact test for candidates
+//     the ray cannot reach; the exact tests are the reference's
+//     single-precision ones, so every hit decision is the reference's.
+//     Skipped candidates would have contributed exactly 0.  The plates use a
+//     fast path that proves "fully traversed" with margins, else the exact
+//     test.  Values that are not hit decisions (solid angle, path inside the
+//     detecting crystal, absorption chord) use closed forms in single
+//     precision.
 //  4. Lanes accumulate with Kahan summation; warp shuffles reduce; the CTA
 //     stages its 8 x brick results in shared memory and writes them out.
 #include <cuda_runtime.h>
@@ -53,6 +61,8 @@ struct WarpLists {
     int plate_begin[kMaxPlates + 1];  // list_h index where each plate's holes start
     unsigned mask_c[kMaxGroup][kLWC]; // per sub-point: candidates after the cone test
     unsigned mask_h[kMaxGroup][kLWH];
+    unsigned pass_c[kLWC];            // per warp pass: candidates the pass's bundle of rays can reach
+    unsigned pass_h[kLWH];
 };
 
 struct __align__(16) PeSmem {
@@ -272,23 +282,37 @@ __device__ __noinline__ float self_path_exact(Vec3 ps, Vec3 qs, Box3 crystal, Bo
     return l1 - l2;
 }
 
+// Sub-cell centre in the detecting crystal's frame (xDs, yDs, zDs) and in the
+// world (q), as the reference computes them (PESysMatGen.cu:606-616).
+struct SubCell {
+    float xDs, yDs, zDs;
+    Vec3 q;
+};
+
+__device__ __forceinline__ SubCell sub_cell(const Detecting& D, const PeSmem& S, int sx, int sy, int sz) {
+    SubCell c;
+    c.xDs = -D.w / 2.0f + S.frac[0][sx] * D.w;
+    c.zDs = -D.h / 2.0f + S.frac[2][sz] * D.h;
+    c.yDs = -D.t / 2.0f + S.frac[1][sy] * D.t;
+    c.q.x = D.cx + (c.xDs * D.cp - c.zDs * D.sp);
+    c.q.z = D.cz + (c.xDs * D.sp + c.zDs * D.cp);
+    c.q.y = D.cy + c.yDs;
+    return c;
+}
+
 // One ray: sub-point p (world) and ps (detecting crystal frame), sub-cell
-// (sx, sy, sz).  mask_c / mask_h: the sub-point's candidates over the warp's
-// lists.  Returns the contribution; in RECORD mode also the hit record.
+// `cell`.  mask_c / mask_h: the sub-point's candidates over the warp's lists;
+// L.pass_c / L.pass_h: the candidates the warp pass's bundle of rays can reach
+// (a superset of those this ray can reach).  Returns the contribution; in
+// RECORD mode also the hit record.
 template <bool RECORD>
 __device__ __forceinline__ float trace_ray(const PEParams& P, const DevGeometry& G, const PeSmem& S,
                                            const WarpLists& L, const unsigned* mask_c, const unsigned* mask_h,
-                                           const Detecting& D, const Vec3& p, const Vec3& ps, int sx, int sy, int sz,
+                                           const Detecting& D, const Vec3& p, const Vec3& ps, const SubCell& cell,
                                            int* rec, int* status, unsigned long long* n_cry,
                                            unsigned long long* n_hole) {
-    // Sub-cell centre, crystal frame then world (PESysMatGen.cu:606-616).
-    const float xDs = -D.w / 2.0f + S.frac[0][sx] * D.w;
-    const float zDs = -D.h / 2.0f + S.frac[2][sz] * D.h;
-    const float yDs = -D.t / 2.0f + S.frac[1][sy] * D.t;
-    Vec3 q;
-    q.x = D.cx + (xDs * D.cp - zDs * D.sp);
-    q.z = D.cz + (xDs * D.sp + zDs * D.cp);
-    q.y = D.cy + yDs;
+    const float xDs = cell.xDs, yDs = cell.yDs, zDs = cell.zDs;
+    const Vec3 q = cell.q;
 
     RaySeg seg;
     seg.p = p;
@@ -315,7 +339,7 @@ __device__ __forceinline__ float trace_ray(const PEParams& P, const DevGeometry&
         float in_holes = 0.0f;
         const int hb = L.plate_begin[m], he = L.plate_begin[m + 1];
         for (int wd = hb >> 5; wd <= ((he - 1) >> 5) && he > hb; ++wd) {
-            unsigned bits = mask_h[wd];
+            unsigned bits = mask_h[wd] & L.pass_h[wd];
             const int lo = hb - (wd << 5), hi = he - (wd << 5);
             if (lo > 0) bits &= ~0u << lo;
             if (hi < 32) bits &= (1u << hi) - 1u;
@@ -343,7 +367,7 @@ __device__ __forceinline__ float trace_ray(const PEParams& P, const DevGeometry&
     // Other crystals among the candidates, each in its own frame (:687-725).
     const int nwc = (L.n_c + 31) >> 5;
     for (int wd = 0; wd < nwc; ++wd) {
-        unsigned bits = mask_c[wd];
+        unsigned bits = mask_c[wd] & L.pass_c[wd];
         while (bits) {
             const int b = __ffs(bits) - 1;
             bits &= bits - 1;
@@ -581,11 +605,23 @@ __device__ __forceinline__ void pe_tile(const PEParams& P, const DevGeometry& G,
         unsigned long long cnt_rays = 0, cnt_cry = 0, cnt_hole = 0, cnt_cone = 0;
         unsigned long long* pc_cry = P.counters ? &cnt_cry : nullptr;
         unsigned long long* pc_hole = P.counters ? &cnt_hole : nullptr;
-        for (int vl = 0; vl < tv; ++vl) {
+        // Entries of fewer than 32 rays go two voxels to a warp pass (P.pair):
+        // the lanes of voxel 0 and voxel 1 are summed apart.
+        const int VP = RECORD ? 1 : P.pair;
+        for (int vl = 0; vl < tv; vl += VP) {
             const int ix = ix0 + vl % P.bx;
             const int iy = iy0 + (vl / P.bx) % P.by;
             const int iz = iz0 + vl / (P.bx * P.by);
-            if (ix >= ix1 || iy >= iy1 || iz >= iz1) continue;
+            const bool valid0 = ix < ix1 && iy < iy1 && iz < iz1;
+            int jx = 0, jy = 0, jz = 0;
+            bool valid1 = false;
+            if (VP == 2 && vl + 1 < tv) {
+                jx = ix0 + (vl + 1) % P.bx;
+                jy = iy0 + ((vl + 1) / P.bx) % P.by;
+                jz = iz0 + (vl + 1) / (P.bx * P.by);
+                valid1 = jx < ix1 && jy < iy1 && jz < iz1;
+            }
+            if (!valid0 && !valid1) continue;
             int rec_slot = -1;
             if (RECORD) {
                 const long long vox = ((long long)iz * P.ny + iy) * P.nx + ix;
@@ -594,11 +630,19 @@ __device__ __forceinline__ void pe_tile(const PEParams& P, const DevGeometry& G,
                 if (rec_slot < 0) continue;
             }
             float acc = 0.0f, comp = 0.0f;
+            int lane_vox = 0;
             if (absorbing) {
                 // Voxel-level candidate lists: staged crystals/holes the bundle from
-                // this voxel's sub-points to the crystal can reach.
+                // the sub-points of this voxel (or voxel pair) to the crystal can reach.
+                Box3 Avox = valid0 ? point_box_of(ix, iy, iz, ix + 1, iy + 1, iz + 1)
+                                   : point_box_of(jx, jy, jz, jx + 1, jy + 1, jz + 1);
+                if (valid0 && valid1) {
+                    const Box3 B2 = point_box_of(jx, jy, jz, jx + 1, jy + 1, jz + 1);
+                    Avox = Box3{fminf(Avox.x1, B2.x1), fminf(Avox.y1, B2.y1), fminf(Avox.z1, B2.z1),
+                                fmaxf(Avox.x2, B2.x2), fmaxf(Avox.y2, B2.y2), fmaxf(Avox.z2, B2.z2)};
+                }
                 {
-                    const Bundle bv = make_bundle(point_box_of(ix, iy, iz, ix + 1, iy + 1, iz + 1), D.world);
+                    const Bundle bv = make_bundle(Avox, D.world);
                     int cnt = 0;
                     for (int k0 = 0; k0 < n_c; k0 += 32) {
                         const int k = k0 + lane;
@@ -631,11 +675,16 @@ __device__ __forceinline__ void pe_tile(const PEParams& P, const DevGeometry& G,
                     __syncwarp();
                 }
                 const int lc = L.n_c, lh = L.n_h;
-                for (int s0 = 0; s0 < P.n_sv; s0 += P.group) {
-                    const int gn = min(P.group, P.n_sv - s0);
-                    // Candidate masks for sub-points s0 .. s0+gn-1 (cone test on the lists).
+                const int nwc = (lc + 31) >> 5, nwh = (lh + 31) >> 5;
+                // points of the pass(es): sub-points of voxel 0, then of voxel 1
+                const int n_pts = VP * P.n_sv;
+                for (int s0 = 0; s0 < n_pts; s0 += P.group) {
+                    const int gn = min(P.group, n_pts - s0);
+                    // Candidate masks for points s0 .. s0+gn-1 (cone test on the lists).
                     for (int j = 0; j < gn; ++j) {
-                        const Vec3 p = subpoint_of(P, ix, iy, iz, s0 + j);
+                        const int u = (VP == 1) ? 0 : (s0 + j) / P.n_sv;
+                        const Vec3 p = u == 0 ? subpoint_of(P, ix, iy, iz, s0 + j)
+                                              : subpoint_of(P, jx, jy, jz, s0 + j - P.n_sv);
                         const ConeSelf cs = cone_self(D, p);
                         const Bundle bp = make_bundle(Box3{p.x, p.y, p.z, p.x, p.y, p.z}, D.world);
                         for (int i0 = 0; i0 < lc; i0 += 32) {
@@ -673,26 +722,87 @@ __device__ __forceinline__ void pe_tile(const PEParams& P, const DevGeometry& G,
                         }
                     }
                     __syncwarp();
+                    // Rays of the group, ordered (sub-cell column, sub-point, depth
+                    // sub-cell) and dealt 32 to a warp pass: a pass traces the depth
+                    // cells of one column (or a few) from neighbouring sub-points,
+                    // rays that run almost together through the plates and the
+                    // crystals in front, so the lanes meet the same candidates.
+                    const int cb = gn * P.dY;                  // rays per sub-cell column
+                    const float inv_cb = 1.0f / (float)cb;
                     const int nr = gn * P.n_sc;
                     for (int q0 = 0; q0 < nr; q0 += 32) {
-                        const int q = q0 + lane;
-                        if (q < nr) {
-                            const int j = (gn == 1) ? 0 : fast_div(q, P.n_sc, P.inv_n_sc);
-                            const int c = q - j * P.n_sc;
-                            const int sz = fast_div(c, P.dX * P.dY, P.inv_dXdY);
-                            const int rem = c - sz * P.dX * P.dY;
-                            const int sx = fast_div(rem, P.dY, P.inv_dY);
-                            const int sy = rem - sx * P.dY;
-                            const Vec3 p = subpoint_of(P, ix, iy, iz, s0 + j);
+                        const int e = q0 + lane;
+                        bool active = e < nr;
+                        int j = 0, sx = 0, sy = 0, sz = 0, u = 0;
+                        if (active) {
+                            const int col = fast_div(e, cb, inv_cb);
+                            const int r = e - col * cb;
+                            j = fast_div(r, P.dY, P.inv_dY);
+                            sy = r - j * P.dY;
+                            sz = fast_div(col, P.dX, P.inv_dX);
+                            sx = col - sz * P.dX;
+                            if (VP == 2) {
+                                u = (s0 + j) / P.n_sv;
+                                active = u == 0 ? valid0 : valid1;
+                                lane_vox = u;
+                            }
+                        }
+                        const SubCell cell = sub_cell(D, S, sx, sy, sz);
+                        // The pass's bundle: from the voxel's sub-point box to the
+                        // box of its rays' sub-cell centres.
+                        float bx1 = active ? cell.q.x : 3.0e38f, bx2 = active ? cell.q.x : -3.0e38f;
+                        float by1 = active ? cell.q.y : 3.0e38f, by2 = active ? cell.q.y : -3.0e38f;
+                        float bz1 = active ? cell.q.z : 3.0e38f, bz2 = active ? cell.q.z : -3.0e38f;
+                        for (int o = 16; o > 0; o >>= 1) {
+                            bx1 = fminf(bx1, __shfl_xor_sync(0xffffffffu, bx1, o));
+                            bx2 = fmaxf(bx2, __shfl_xor_sync(0xffffffffu, bx2, o));
+                            by1 = fminf(by1, __shfl_xor_sync(0xffffffffu, by1, o));
+                            by2 = fmaxf(by2, __shfl_xor_sync(0xffffffffu, by2, o));
+                            bz1 = fminf(bz1, __shfl_xor_sync(0xffffffffu, bz1, o));
+                            bz2 = fmaxf(bz2, __shfl_xor_sync(0xffffffffu, bz2, o));
+                        }
+                        const Bundle bq = make_bundle(Avox, Box3{bx1, by1, bz1, bx2, by2, bz2});
+                        // Narrow the group's candidates (any sub-point's mask) to
+                        // those the pass can reach; a candidate dropped here is one
+                        // that no ray of the pass can reach, i.e. one trace_ray would
+                        // skip by its own window test.
+                        for (int w = 0; w < nwc; ++w) {
+                            unsigned u = 0u;
+                            for (int jj = 0; jj < gn; ++jj) u |= L.mask_c[jj][w];
+                            bool pass = false;
+                            if ((u >> lane) & 1u) {
+                                const int k = L.list_c[(w << 5) + lane];
+                                pass = bundle_hit(bq, box_of(S.c_lo[k], S.c_hi[k]));
+                            }
+                            const unsigned bal = __ballot_sync(0xffffffffu, pass);
+                            if (lane == 0) L.pass_c[w] = bal;
+                        }
+                        for (int w = 0; w < nwh; ++w) {
+                            unsigned u = 0u;
+                            for (int jj = 0; jj < gn; ++jj) u |= L.mask_h[jj][w];
+                            bool pass = false;
+                            if ((u >> lane) & 1u) {
+                                const int k = L.list_h[(w << 5) + lane];
+                                pass = bundle_hit(bq, hole_box(S.h_a[k], S.h_b[k]));
+                            }
+                            const unsigned bal = __ballot_sync(0xffffffffu, pass);
+                            if (lane == 0) L.pass_h[w] = bal;
+                        }
+                        __syncwarp();
+                        if (active) {
+                            const Vec3 p = u == 0 ? subpoint_of(P, ix, iy, iz, s0 + j)
+                                                  : subpoint_of(P, jx, jy, jz, s0 + j - P.n_sv);
                             Vec3 ps;
                             ps.x = (p.x - D.cx) * D.cm - (p.z - D.cz) * D.sm;
                             ps.y = p.y - D.cy;
                             ps.z = (p.x - D.cx) * D.sm + (p.z - D.cz) * D.cm;
                             int* rec = nullptr;
-                            if (RECORD)
+                            if (RECORD) {
+                                const int c = (sz * P.dX + sx) * P.dY + sy;   // the oracle's sub-cell order
                                 rec = P.rec_out + ((long long)rec_slot * P.n_sv * P.n_sc + (long long)(s0 + j) * P.n_sc + c) *
                                                       kRecWords;
-                            const float v = trace_ray<RECORD>(P, G, S, L, L.mask_c[j], L.mask_h[j], D, p, ps, sx, sy, sz,
+                            }
+                            const float v = trace_ray<RECORD>(P, G, S, L, L.mask_c[j], L.mask_h[j], D, p, ps, cell,
                                                               rec, P.status, pc_cry, pc_hole);
                             if (P.counters) ++cnt_rays;
                             // Kahan summation of the lane's rays.
@@ -701,13 +811,23 @@ __device__ __forceinline__ void pe_tile(const PEParams& P, const DevGeometry& G,
                             comp = (t - acc) - y;
                             acc = t;
                         }
+                        __syncwarp();
                     }
                     __syncwarp();
                 }
             }
             float v = acc - comp;
+            float v1 = 0.0f;
+            if (VP == 2) {
+                v1 = lane_vox == 1 ? v : 0.0f;
+                v = lane_vox == 0 ? v : 0.0f;
+                for (int o = 16; o > 0; o >>= 1) v1 += __shfl_xor_sync(0xffffffffu, v1, o);
+            }
             for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-            if (lane == 0) S.out[warp][vl] = v * P.inv_sv;
+            if (lane == 0) {
+                if (valid0) S.out[warp][vl] = v * P.inv_sv;
+                if (valid1) S.out[warp][vl + 1] = v1 * P.inv_sv;
+            }
         }
         if (P.counters) {
             for (int o = 16; o > 0; o >>= 1) {

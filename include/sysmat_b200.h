@@ -109,10 +109,11 @@ typedef struct sm_pe_options {
     int sc[3];          /* crystal sub-cells (x, y = depth, z); summed           */
     int tile_voxels[3]; /* voxel brick per CTA; 0 = default (8 x 4 x 4)          */
     int flags;          /* SM_PE_AUTOTUNE: choose tile_voxels and group with sm_pe_autotune */
-    int group;          /* voxel sub-points a warp traces per pass, i.e. group * sc rays per
-                           pass, group * sc / 32 per lane; 0 = the fewest that fill a warp
-                           (at most 4).  Groups with group * sc[0]*sc[1]*sc[2] a multiple
-                           of 32 give identical results. */
+    int group;          /* voxel sub-points whose rays a warp traces together (each lane
+                           traces group * sc[0]*sc[1]*sc[2] / 32 of them); 0 = 32 / sc[1],
+                           at most 8: one warp pass then covers one column of depth
+                           sub-cells.  It changes which lane sums which ray, so the
+                           rounding of the sums, never a hit decision. */
 } sm_pe_options;
 
 enum { SM_PE_AUTOTUNE = 1 };

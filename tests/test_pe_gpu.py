@@ -150,6 +150,18 @@ def test_tiling_slabs_and_rows_do_not_change_results(ctx):
     g.close()
 
 
+def test_voxel_pairs_do_not_change_results(ctx):
+    """Entries of at most 16 rays (voxel centre x 2x4x2 sub-cells) go two voxels
+    to a warp pass; which neighbour a voxel is paired with (it depends on the
+    brick) changes no value, and a voxel alone in a pass gives the same."""
+    p = configs.tiny(layers=3)
+    g = sysmat_b200.Geometry(ctx, p)
+    full = g.pe()
+    for tile in [(1, 1, 1), (3, 2, 1), (4, 4, 4), (2, 3, 3), (1, 4, 2)]:
+        assert np.array_equal(g.pe(opts=g.options(tile_voxels=tile)), full), tile
+    g.close()
+
+
 def test_legacy_pesysmatgen_slabs_match_api(ctx):
     """PESysMatGen with the reference CLI's slab side channel reproduces the
     sm API in reference mode (voxel centre, 8 x 16 x 8 sub-cells)."""

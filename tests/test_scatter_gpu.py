@@ -8,13 +8,13 @@ full-size workload.
 
 Tolerances, relative error on nonzero entries:
 * bitmaps: identical words (the reference's single-precision test);
-* values vs FP64: median <= 1e-4 and 99th percentile <= 1e-3.  The maximum is
-  held to 2e-2: an entry sums up to N x points terms, and a term sits on one of
-  the reference's hard edges (the 2-sigma energy-window cut, the floor in the
-  0.01 rad Klein-Nishina rectangle sum, the theta_min = 0 switch) where the
-  FP32 and FP64 decisions can differ; the reference's own FP32 kernel moves
-  such entries by the same amount.  The fraction of entries above 1e-3 is
-  held to 1%.
+* values vs FP64: median <= 1e-5, 99th percentile <= 1e-4, maximum <= 1e-3
+  (measured on these fixtures and samples: median ~1e-7, maximum ~1e-5).  An
+  entry sums up to N x points terms, and a term that sits on one of the
+  reference's hard edges (the 2-sigma energy-window cut, the floor in the
+  0.01 rad Klein-Nishina rectangle sum, the theta_min = 0 switch) can be decided
+  differently in FP32 and FP64; the maximum leaves room for one such term, and
+  at most 1% of the entries may exceed 1e-4.
 * zero pattern: an entry is zero exactly when the oracle's is, except where
   the oracle's value is below 1e-6 of the row's maximum.
 """
@@ -31,9 +31,9 @@ from sysmat_b200 import configs
 
 pytestmark = pytest.mark.gpu
 
-MEDIAN = 1e-4
-P99 = 1e-3
-MAX = 2e-2
+MEDIAN = 1e-5
+P99 = 1e-4
+MAX = 1e-3
 FRAC_ABOVE = 0.01
 
 
@@ -49,12 +49,12 @@ def check_values(got, ref, what):
     ref = np.asarray(ref, np.float64)
     err = rel_err(got, ref)
     assert err.size > 0, what
-    stats = "median %.3g p99 %.3g max %.3g above1e-3 %.4f (n=%d)" % (
-        np.median(err), np.quantile(err, 0.99), err.max(), (err > 1e-3).mean(), err.size)
+    stats = "median %.3g p99 %.3g max %.3g above1e-4 %.4f (n=%d)" % (
+        np.median(err), np.quantile(err, 0.99), err.max(), (err > 1e-4).mean(), err.size)
     assert np.median(err) <= MEDIAN, what + ": " + stats
     assert np.quantile(err, 0.99) <= P99, what + ": " + stats
     assert err.max() <= MAX, what + ": " + stats
-    assert (err > 1e-3).mean() <= FRAC_ABOVE, what + ": " + stats
+    assert (err > 1e-4).mean() <= FRAC_ABOVE, what + ": " + stats
     scale = np.max(np.abs(ref)) if ref.size else 0.0
     flip = (got == 0) != (ref == 0)
     assert not np.any(flip & (np.abs(ref) > 1e-6 * scale)), what + ": zero pattern differs"
