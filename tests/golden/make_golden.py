@@ -186,10 +186,28 @@ def shipped_fixture(tree: str, name: str, prefix: str):
     rng = np.random.default_rng(zlib.crc32(("shipped_" + name).encode()))
     rotations = (0,) if p.n_rotations == 1 else (0, p.n_rotations // 2, p.n_rotations - 1)
     rows_all, vox_all, rot_all = [], [], []
-    for rot in rotations:
+    extra = {}
+    if p.n_crystals == 1:
+        # One crystal, seen from few voxels: its whole file, every rotation, from the
+        # restatement (pinned bit for bit to the reference's code); the nonzero cells
+        # are the golden zero pattern and a sample of them gets the reference's values.
+        nonzero = []
+        for rot in range(p.n_rotations):
+            v = oracle_py.oracle_pe_entries(p, np.zeros(p.n_voxels, np.int64), np.arange(p.n_voxels), "fp32",
+                                            rotation=rot)
+            nonzero.append(rot * p.n_voxels + np.flatnonzero(v))
+        nonzero = np.concatenate(nonzero)
+        extra["nonzero_cells"] = nonzero
+        pick = rng.choice(nonzero, min(96, nonzero.size), replace=False) if nonzero.size else nonzero
+        rows_all.append(np.zeros(pick.size, np.int64))
+        vox_all.append(pick % p.n_voxels)
+        rot_all.append(pick // p.n_voxels)
+        rotations = tuple(int(r) for r in np.unique(pick // p.n_voxels)) + rotations
+    for rot in sorted(set(rotations)) if p.n_crystals > 1 else (0, p.n_rotations // 2, p.n_rotations - 1):
         for r0, r1 in SHIPPED_ROW_BLOCKS[name]:
             for row in range(r0, r1):
-                cand = rng.choice(p.n_voxels, 256, replace=False)
+                # a geometry with one crystal sees it from few voxels: look at more of them
+                cand = rng.choice(p.n_voxels, 256 if p.n_crystals > 1 else 8192, replace=False)
                 v = oracle_py.oracle_pe_entries(p, np.full(cand.size, row), cand, "fp32", rotation=rot)
                 top = cand[np.argsort(-v)[:3]]
                 nz = cand[v != 0]
@@ -204,14 +222,15 @@ def shipped_fixture(tree: str, name: str, prefix: str):
     rot = np.concatenate(rot_all)
     f32 = np.zeros(rows.size)
     f64 = np.zeros(rows.size)
-    for r in rotations:
+    for r in np.unique(rot):
+        r = int(r)
         m = rot == r
         f32[m] = oracle_py.ref_pe_entries(p, rows[m], vox[m], "f32", rotation=int(r))
         f64[m] = oracle_py.ref_pe_entries(p, rows[m], vox[m], "f64", rotation=int(r))
     np.savez_compressed(os.path.join(HERE, "pe_shipped_%s.npz" % name), collimator=col, detector=det, image=img,
                         physics=phy, sv=np.asarray(p.sv), sc=np.asarray(p.sc), rows=rows, voxels=vox, rotation=rot,
                         ref_f32=f32, ref_f64=f64,
-                        row_blocks=np.asarray(SHIPPED_ROW_BLOCKS[name], dtype=np.int64))
+                        row_blocks=np.asarray(SHIPPED_ROW_BLOCKS[name], dtype=np.int64), **extra)
     print("pe_shipped_%s: %d crystals, %d holes, grid %s, %d cells, nonzero %d" % (
         name, p.n_crystals, p.n_holes, p.grid, rows.size, int((f64 != 0).sum())))
 

@@ -62,21 +62,31 @@ def _pe_case():
 
 
 def test_reference_pegen_host_on_library_matches_reference_build(tmp_path):
-    ours_bin = _binary("PEGen_CircularHole.sysmat_b200")
-    ref_bin = _binary("PEGen_CircularHole.ref")
+    """Against the reference's GPU build without multiply-add contraction (the
+    single-precision semantics of its source, which the golden vectors pin):
+    identical zeros and every entry within 1e-4.  Against its default build,
+    where nvcc fuses multiply-adds and so decides some rays that graze a hole
+    wall the other way (a ray through a hole instead of 5 mm of tungsten moves
+    an almost fully blocked entry by orders of magnitude): identical zeros,
+    median within 1e-5, and at most 2 % of the entries beyond 1e-4."""
+    binaries = {"ours": _binary("PEGen_CircularHole.sysmat_b200"), "ref": _binary("PEGen_CircularHole.ref"),
+                "ref_nofma": _binary("PEGen_CircularHole.ref_nofma")}
     p = _pe_case()
     out = {}
-    for tag, binary in (("ours", ours_bin), ("ref", ref_bin)):
+    for tag, binary in binaries.items():
         d = tmp_path / tag
         p.write_dat(str(d))
         _run(binary, d, ["-cuda", "0"])
         out[tag] = np.fromfile(d / _shift_name("PE_SysMat", p), np.float32)
     N, V = p.n_crystals, p.n_voxels
-    assert out["ours"].size == out["ref"].size == 2 * N * V
+    assert out["ours"].size == out["ref"].size == out["ref_nofma"].size == 2 * N * V
     assert (out["ref"] != 0).sum() > 0.1 * out["ref"].size
+    assert np.array_equal(out["ours"] == 0, out["ref_nofma"] == 0)
+    err = rel_err(out["ours"], out["ref_nofma"])
+    assert err.max() <= 1e-4, err.max()
     assert np.array_equal(out["ours"] == 0, out["ref"] == 0)
     err = rel_err(out["ours"], out["ref"])
-    assert err.max() <= 1e-4, err.max()
+    assert np.median(err) <= 1e-5 and (err > 1e-4).mean() <= 0.02, (np.median(err), (err > 1e-4).mean())
 
 
 def test_reference_scattergen_host_on_library_matches_reference_build(tmp_path):
