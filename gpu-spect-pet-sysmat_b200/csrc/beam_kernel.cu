@@ -65,19 +65,7 @@ __global__ void __launch_bounds__(kBeamThreads) beam_rows_kernel(const float* __
         if (VEC) {
             const float4* row4 = reinterpret_cast<const float4*>(row);
             const long long n4 = V >> 2;
-            long long i = tid;
-            // four independent 128-bit loads in flight per thread
-            for (; i + 3 * kBeamThreads < n4; i += 4 * kBeamThreads) {
-                float4 v[4];
-#pragma unroll
-                for (int u = 0; u < 4; ++u) v[u] = __ldg(row4 + i + u * kBeamThreads);
-#pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    mx = fmaxf(fmaxf(mx, fmaxf(v[u].x, v[u].y)), fmaxf(v[u].z, v[u].w));
-                    s += ((double)v[u].x + (double)v[u].y) + ((double)v[u].z + (double)v[u].w);
-                }
-            }
-            for (; i < n4; i += kBeamThreads) {
+            for (long long i = tid; i < n4; i += kBeamThreads) {
                 const float4 v = __ldg(row4 + i);
                 mx = fmaxf(fmaxf(mx, fmaxf(v.x, v.y)), fmaxf(v.z, v.w));
                 s += ((double)v.x + (double)v.y) + ((double)v.z + (double)v.w);
@@ -117,19 +105,7 @@ __global__ void __launch_bounds__(kBeamThreads) beam_rows_kernel(const float* __
         if (VEC) {
             const float4* row4 = reinterpret_cast<const float4*>(row);
             const long long n4 = V >> 2;
-            long long i = tid;
-            for (; i + 3 * kBeamThreads < n4; i += 4 * kBeamThreads) {
-                float4 v[4];
-#pragma unroll
-                for (int u = 0; u < 4; ++u) v[u] = __ldg(row4 + i + u * kBeamThreads);
-#pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    const int b0 = v[u].x > thr, b1 = v[u].y > thr, b2 = v[u].z > thr, b3 = v[u].w > thr;
-                    c += b0 + b1 + b2 + b3;
-                    if (mrow) reinterpret_cast<char4*>(mrow)[i + u * kBeamThreads] = make_char4(b0, b1, b2, b3);
-                }
-            }
-            for (; i < n4; i += kBeamThreads) {
+            for (long long i = tid; i < n4; i += kBeamThreads) {
                 const float4 v = __ldg(row4 + i);
                 const int b0 = v.x > thr, b1 = v.y > thr, b2 = v.z > thr, b3 = v.w > thr;
                 c += b0 + b1 + b2 + b3;
@@ -167,20 +143,7 @@ __global__ void __launch_bounds__(kBeamThreads) beam_mpxi_kernel(const float* __
     const long long r1 = r0 + rows_per_block < rows ? r0 + rows_per_block : rows;
     const int nc = V - c0 >= 4 ? 4 : (int)(V - c0);
     unsigned u[4] = {0u, 0u, 0u, 0u};
-    long long r = r0;
-    if (FROM_MASK && VEC && nc == 4) {
-        // four rows' mask words in flight per thread
-        for (; r + 3 < r1; r += 4) {
-            char4 b[4];
-#pragma unroll
-            for (int k = 0; k < 4; ++k) b[k] = *reinterpret_cast<const char4*>(mask + (r + k) * ldm + c0);
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                u[0] += b[k].x; u[1] += b[k].y; u[2] += b[k].z; u[3] += b[k].w;
-            }
-        }
-    }
-    for (; r < r1; ++r) {
+    for (long long r = r0; r < r1; ++r) {
         if (FROM_MASK) {
             const signed char* m = mask + r * ldm + c0;
             if (VEC && nc == 4) {
