@@ -339,18 +339,13 @@ __device__ __forceinline__ float trace_ray(const PEParams& P, const DevGeometry&
         float in_holes = 0.0f;
         const int hb = L.plate_begin[m], he = L.plate_begin[m + 1];
         for (int wd = hb >> 5; wd <= ((he - 1) >> 5) && he > hb; ++wd) {
-            // walk the pass's candidates (the same for every lane of the pass, so
-            // the lanes stay together and read the same records); a lane skips
-            // those outside its own sub-point's mask
-            unsigned bits = L.pass_h[wd];
-            const unsigned mine = mask_h[wd];
+            unsigned bits = mask_h[wd] & L.pass_h[wd];
             const int lo = hb - (wd << 5), hi = he - (wd << 5);
             if (lo > 0) bits &= ~0u << lo;
             if (hi < 32) bits &= (1u << hi) - 1u;
             while (bits) {
                 const int b = __ffs(bits) - 1;
                 bits &= bits - 1;
-                if (!((mine >> b) & 1u)) continue;
                 const int k = L.list_h[(wd << 5) + b];
                 const float4 ha = S.h_a[k], hbv = S.h_b[k];
                 if (!ray_may_hit(seg, hole_box(ha, hbv))) continue;
@@ -372,12 +367,10 @@ __device__ __forceinline__ float trace_ray(const PEParams& P, const DevGeometry&
     // Other crystals among the candidates, each in its own frame (:687-725).
     const int nwc = (L.n_c + 31) >> 5;
     for (int wd = 0; wd < nwc; ++wd) {
-        unsigned bits = L.pass_c[wd];
-        const unsigned mine = mask_c[wd];
+        unsigned bits = mask_c[wd] & L.pass_c[wd];
         while (bits) {
             const int b = __ffs(bits) - 1;
             bits &= bits - 1;
-            if (!((mine >> b) & 1u)) continue;
             const int k = L.list_c[(wd << 5) + b];
             if (!ray_may_hit(seg, box_of(S.c_lo[k], S.c_hi[k]))) continue;
             if (n_cry) ++*n_cry;
