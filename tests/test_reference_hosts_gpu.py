@@ -2,22 +2,32 @@
 
 oracle/Makefile (target ``ref-cli``) compiles the reference's
 ``PEGen_RayTracing_CircularHole/PEGen_CircularHole.cpp`` and
-``ScatterGen_RayTracing_CircularHole/ScatterGen_CircularHole.cpp`` twice, with
-no source change:
+``ScatterGen_RayTracing_CircularHole/ScatterGen_CircularHole.cpp`` with no
+source change:
 
 * ``*.sysmat_b200``: linked against libsysmat_b200.so, the way a maintainer
   switches the reference to this library (the ``PESysMatGen`` / ``scatter``
   drop-ins, include/sysmat_b200.h);
-* ``*.ref``: linked against the reference's own ``PESysMatGen.cu`` /
-  ``scatter.cu`` built for sm_100a.
+* ``*.ref`` / ``*.ref_nofma``: linked against the reference's own
+  ``PESysMatGen.cu`` / ``scatter.cu`` built for sm_100a (nvcc's default
+  multiply-add contraction, and without it).
 
-Both run in their own working directory on the same ``Params_*.dat`` and must
-write the same files: the PE sysmat with identical zero patterns and values
-within 1e-4 relative (the two implementations take the same single-precision
-hit decisions and differ only in value arithmetic), the geometry bitmaps bit
-for bit, and the scatter sysmat within the tolerance of the scatter parity
-tests (the reference's scatter kernels add with float atomics in no fixed
-order).
+PE: the file the reference host writes through this library is compared,
+entry by entry, with the reference's kernel code evaluated on the host cores
+(oracle/_ref/libref_pe_f32.so: PESysMatGen.cu compiled by g++, IEEE single, no
+contraction) and with the FP64 oracle.  The reference's own GPU build is run
+on the same files as well.  On B200 that build disagrees with its own host
+build on about 40 % of the nonzero entries of these geometries, always in the
+same direction: the entry comes out ~1e-6 of the host value, i.e. the rays
+cross the full tungsten thickness instead of a hole (the file's zero pattern is
+unchanged).  The deviation is the same with and without contraction, so it is
+not rounding; this library follows the host build.  The test therefore pins
+this library to the host build on every entry, and to the GPU build on the
+entries where that build agrees with its own host build.
+
+Scatter: the geometry bitmaps bit for bit, and the scatter sysmat within the
+tolerance of the scatter parity tests (the reference's scatter kernels add
+with float atomics in no fixed order).
 """
 import os
 import shutil
@@ -26,12 +36,16 @@ import subprocess
 import numpy as np
 import pytest
 
+import oracle_py
 from helpers import rel_err
 from sysmat_b200 import configs
 
 pytestmark = pytest.mark.gpu
 
 REF_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "..", "oracle", "_ref")
+# |ours - host| <= 1e-4 |host| and |gpu - host| <= 1e-4 |host| bound |ours - gpu| by ~2e-4 |gpu|
+MAX_VS_HOST = 1e-4
+MAX_VS_AGREEING_GPU = 2e-4
 
 
 def _binary(name):
@@ -54,13 +68,14 @@ def _shift_name(prefix, p):
 def _pe_case(rotated):
     """6 z-planes (the reference host's 4-plane slab loop ends on a 2-plane
     slab); `rotated` adds crystal rotations, a second image rotation and an FOV
-    shift, otherwise every angle is 0 (cos and sin exact on any device)."""
+    shift, otherwise every angle is 0.  Reference sub-cells 8 x 16 x 8."""
     p = configs.tiny(seed=4, rotated=True) if rotated else configs.tiny(seed=4)
     p.image = p.image.copy()
     p.image[2] = 6
     p.image[30] = 6
     p.image[6] = 2 if rotated else 1
     p.image[7] = np.float32(0.1) if rotated else np.float32(0.0)
+    p.sv, p.sc = (1, 1, 1), (8, 16, 8)
     return p
 
 
@@ -70,8 +85,23 @@ def _run_hosts(p, tmp_path, names):
         d = tmp_path / tag
         p.write_dat(str(d))
         _run(_binary("PEGen_CircularHole." + tag), d, ["-cuda", "0"])
-        out[tag] = np.fromfile(d / _shift_name("PE_SysMat", p), np.float32)
+        a = np.fromfile(d / _shift_name("PE_SysMat", p), np.float32)
+        assert a.size == p.n_rotations * p.n_crystals * p.n_voxels, tag
+        out[tag] = a.reshape(p.n_rotations, p.n_crystals, p.n_voxels)
     return out
+
+
+def _host_build(p):
+    """The reference's kernel code on the host cores, every entry of every rotation."""
+    if not oracle_py.ref_available("pe_f32"):
+        pytest.skip("the reference's host build is not built")
+    N, V = p.n_crystals, p.n_voxels
+    rows, vox = np.repeat(np.arange(N), V), np.tile(np.arange(V), N)
+    host = np.stack([oracle_py.ref_pe_entries(p, rows, vox, "f32", rotation=r).reshape(N, V)
+                     for r in range(p.n_rotations)])
+    fp64 = np.stack([oracle_py.oracle_pe_entries(p, rows, vox, "fp64", rotation=r).reshape(N, V)
+                     for r in range(p.n_rotations)])
+    return host, fp64
 
 
 def _stats(err):
@@ -79,38 +109,43 @@ def _stats(err):
         np.median(err), np.quantile(err, 0.99), err.max(), (err > 1e-4).mean(), err.size)
 
 
-def test_reference_pegen_host_on_library_matches_reference_build(tmp_path):
-    """Unrotated crystals: the same file as the reference's own GPU build, with
-    and without multiply-add contraction -- identical zeros, every entry within
-    1e-4 (the two take the same single-precision hit decisions)."""
-    p = _pe_case(rotated=False)
+@pytest.mark.parametrize("rotated", [False, True], ids=["zero_angles", "rotated"])
+def test_reference_pegen_host_on_library_matches_reference_kernel_code(tmp_path, rotated):
+    """Every entry of the file the reference host writes through this library
+    matches the reference's kernel code (host build): identical zeros, each
+    entry within 1e-4; against FP64 median <= 1e-4, max <= 1e-3."""
+    p = _pe_case(rotated)
+    ours = _run_hosts(p, tmp_path, ("sysmat_b200",))["sysmat_b200"]
+    host, fp64 = _host_build(p)
+    assert (ours != 0).sum() > 0.1 * ours.size
+    assert np.array_equal(ours == 0, host == 0)
+    err = rel_err(ours, host)
+    assert err.max() <= MAX_VS_HOST, _stats(err)
+    e64 = rel_err(ours, fp64)
+    assert np.median(e64) <= 1e-4 and e64.max() <= 1e-3, _stats(e64)
+
+
+@pytest.mark.parametrize("rotated", [False, True], ids=["zero_angles", "rotated"])
+def test_reference_pegen_gpu_build_where_it_agrees_with_its_host_build(tmp_path, rotated):
+    """The reference's GPU build (with and without contraction) on the same
+    files: identical zero patterns; on every entry where that build agrees with
+    the reference's host build, this library agrees with it too.  The share of
+    entries where the GPU build departs from its own host build is reported."""
+    p = _pe_case(rotated)
     out = _run_hosts(p, tmp_path, ("sysmat_b200", "ref", "ref_nofma"))
-    N, V = p.n_crystals, p.n_voxels
+    host, _ = _host_build(p)
     ours = out["sysmat_b200"]
-    assert ours.size == N * V and (ours != 0).sum() > 0.1 * ours.size
+    report = []
     for tag in ("ref", "ref_nofma"):
-        assert out[tag].size == ours.size
-        assert np.array_equal(ours == 0, out[tag] == 0), tag
-        err = rel_err(ours, out[tag])
-        assert err.max() <= 1e-4, tag + ": " + _stats(err)
-
-
-def test_reference_pegen_host_rotated_crystals(tmp_path):
-    """Rotated crystals and image rotations: the reference's GPU build takes its
-    cos / sin from the CUDA device library, the golden vectors and this library
-    from the host's (the tables are derived on the host); the two differ in the
-    last bit for some angles, which moves crystal corners and voxel centres by
-    an ulp and flips the decisions of rays that graze a hole wall (a ray through
-    a hole instead of the plate moves an almost blocked entry by orders of
-    magnitude).  Identical zeros, median within 1e-5, and at most 2 % of the
-    entries beyond 1e-4."""
-    p = _pe_case(rotated=True)
-    out = _run_hosts(p, tmp_path, ("sysmat_b200", "ref_nofma"))
-    ours, ref = out["sysmat_b200"], out["ref_nofma"]
-    assert ours.size == ref.size == 2 * p.n_crystals * p.n_voxels
-    assert np.array_equal(ours == 0, ref == 0)
-    err = rel_err(ours, ref)
-    assert np.median(err) <= 1e-5 and (err > 1e-4).mean() <= 0.02, _stats(err)
+        gpu = out[tag]
+        assert np.array_equal(ours == 0, gpu == 0), tag
+        nz = gpu != 0
+        agrees = np.abs(gpu - host) <= MAX_VS_HOST * np.abs(host)
+        assert agrees[nz].mean() > 0.3, tag
+        err = np.abs(ours - gpu)[agrees & nz] / np.abs(gpu[agrees & nz])
+        assert err.max() <= MAX_VS_AGREEING_GPU, tag + ": " + _stats(err)
+        report.append("%s departs from its host build on %.1f %% of nonzero entries" % (tag, 100 * (1 - agrees[nz].mean())))
+    print("; ".join(report))
 
 
 def test_reference_scattergen_host_on_library_matches_reference_build(tmp_path):
