@@ -39,9 +39,12 @@ sys.path.insert(0, os.path.join(ROOT, "gpu-spect-pet-sysmat_b200"))
 
 SLAB_Z = 4
 L2_FLUSH_BYTES = 256 << 20
-# DRAM traffic of one full pe_large slab launch (6400 x 16384 entries), read +
-# write, measured by ncu; None until measured for the current kernel.
-PE_LARGE_SLAB_DRAM_BYTES = None
+# DRAM traffic of one full pe_large slab launch (6400 x 16384 entries):
+# dram__bytes_read.sum 70.51 MB + dram__bytes_write.sum 580.14 MB from one
+# single-pass ncu capture of pe_trace_kernel on B200.  Algorithmic bytes of the
+# same launch: 4 B per entry of output, 419.4 MB, plus 0.64 MB of tables.
+PE_LARGE_SLAB_DRAM_BYTES = 650.65e6
+PE_LARGE_SLAB_ALGORITHMIC_BYTES = 4 * 6400 * 16384 + 2 * 4 * 80000
 
 # FP32 operations per unit of work, counted from the tracer's source
 # (gpu-spect-pet-sysmat_b200/csrc/tracer.cuh, pe_kernel.cu): add/sub/mul/fma
@@ -413,6 +416,7 @@ def run_ours(args, world, rank, local):
             "gpu_launches": args.steps,
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
                          "frac": achieved / fp32_peak, "traffic": traffic,
+                         "traffic_algorithmic_bytes": PE_LARGE_SLAB_ALGORITHMIC_BYTES if traffic else None,
                          "peak_source": "FP32 issue peak 148 SMs x 128 lanes x 2 FLOP x sm_max %.0f MHz (%s clock)" % (sm_max, peak_src.split()[1]),
                          "work": {"rays": n_rays, "exact_crystal_tests": n_cry, "exact_hole_tests": n_hole,
                                   "cone_tests": n_cone, "flops_per_step": flops},

@@ -21,9 +21,12 @@ build on about 40 % of the nonzero entries of these geometries, always in the
 same direction: the entry comes out ~1e-6 of the host value, i.e. the rays
 cross the full tungsten thickness instead of a hole (the file's zero pattern is
 unchanged).  The deviation is the same with and without contraction, so it is
-not rounding; this library follows the host build.  The test therefore pins
-this library to the host build on every entry, and to the GPU build on the
-entries where that build agrees with its own host build.
+not rounding: the same source built with ``-G`` equals the host build on every
+entry, and so does the optimised build once the zero-fill loop of its 40 KB
+local candidate-hole array (PESysMatGen.cu:485-488) is removed.  This library
+follows the reference's source, so the test pins it to the host build on every
+entry, and to the GPU build on the entries where that build agrees with its
+own host build.
 
 Scatter: the geometry bitmaps bit for bit, and the scatter sysmat within the
 tolerance of the scatter parity tests (the reference's scatter kernels add
