@@ -17,11 +17,14 @@
 //     shared memory.
 //  2. Each warp owns one crystal and walks the brick's voxels.  Per voxel it
 //     narrows the staged set with the same window test for that voxel's
-//     sub-point box and compacts the survivors into a per-warp list.  Per
-//     voxel sub-point it evaluates the reference's candidate cone test on
-//     the list (a float filter decides clear cases; cases within 1e-5 of the
-//     threshold use the reference's exact single-precision expression) and
-//     keeps the result as ballot bitmasks over the list.
+//     sub-point box and compacts the survivors into a per-warp list.  The
+//     reference counts a crystal or hole only when it passes the candidate
+//     cone test of (voxel point, detecting crystal); a candidate that the ray
+//     does not cross contributes nothing either way, so the cone test is taken
+//     per ray and only for candidates with a nonzero chord (a float filter
+//     decides clear cases; cases within 1e-5 of the threshold use the
+//     reference's exact single-precision expression).  Each sub-point's own
+//     cone parameters are computed once per group of sub-points.
 //  3. Lanes trace one ray (sub-point, sub-cell) each.  The rays of a group of
 //     sub-points are ordered (sub-cell column, sub-point, depth sub-cell) and
 //     dealt 32 to a warp pass, so a pass holds rays that run almost together
@@ -59,8 +62,7 @@ struct WarpLists {
     unsigned short list_h[kListH];    // ... and holes (ascending ids)
     int n_c, n_h;
     int plate_begin[kMaxPlates + 1];  // list_h index where each plate's holes start
-    unsigned mask_c[kMaxGroup][kLWC]; // per sub-point: candidates after the cone test
-    unsigned mask_h[kMaxGroup][kLWH];
+    float4 cs[kMaxGroup];             // per sub-point of the group: the detecting crystal's cone (ConeSelf)
     unsigned pass_c[kLWC];            // per warp pass: candidates the pass's bundle of rays can reach
     unsigned pass_h[kLWH];
 };
@@ -301,16 +303,19 @@ __device__ __forceinline__ SubCell sub_cell(const Detecting& D, const PeSmem& S,
 }
 
 // One ray: sub-point p (world) and ps (detecting crystal frame), sub-cell
-// `cell`.  mask_c / mask_h: the sub-point's candidates over the warp's lists;
-// L.pass_c / L.pass_h: the candidates the warp pass's bundle of rays can reach
-// (a superset of those this ray can reach).  Returns the contribution; in
-// RECORD mode also the hit record.
+// `cell`.  L.pass_c / L.pass_h: the candidates the warp pass's bundle of rays
+// can reach (a superset of those this ray can reach).  The reference counts a
+// crystal or hole only when it is among the sub-point's cone candidates
+// (PESysMatGen.cu:506-589); a candidate the ray does not cross adds nothing
+// either way, so the cone test (`csp`: the sub-point's ConeSelf) is taken only
+// for candidates with a nonzero chord.  Returns the contribution; in RECORD
+// mode also the hit record.
 template <bool RECORD>
 __device__ __forceinline__ float trace_ray(const PEParams& P, const DevGeometry& G, const PeSmem& S,
-                                           const WarpLists& L, const unsigned* mask_c, const unsigned* mask_h,
-                                           const Detecting& D, const Vec3& p, const Vec3& ps, const SubCell& cell,
-                                           int* rec, int* status, unsigned long long* n_cry,
-                                           unsigned long long* n_hole) {
+                                           const WarpLists& L, const float4* csp, const Detecting& D, const Vec3& p,
+                                           const Vec3& ps, const SubCell& cell, int* rec, int* status,
+                                           unsigned long long* n_cry, unsigned long long* n_hole,
+                                           unsigned long long* n_cone) {
     const float xDs = cell.xDs, yDs = cell.yDs, zDs = cell.zDs;
     const Vec3 q = cell.q;
 
@@ -339,7 +344,7 @@ __device__ __forceinline__ float trace_ray(const PEParams& P, const DevGeometry&
         float in_holes = 0.0f;
         const int hb = L.plate_begin[m], he = L.plate_begin[m + 1];
         for (int wd = hb >> 5; wd <= ((he - 1) >> 5) && he > hb; ++wd) {
-            unsigned bits = mask_h[wd] & L.pass_h[wd];
+            unsigned bits = L.pass_h[wd];
             const int lo = hb - (wd << 5), hi = he - (wd << 5);
             if (lo > 0) bits &= ~0u << lo;
             if (hi < 32) bits &= (1u << hi) - 1u;
@@ -351,6 +356,13 @@ __device__ __forceinline__ float trace_ray(const PEParams& P, const DevGeometry&
                 if (!ray_may_hit(seg, hole_box(ha, hbv))) continue;
                 if (n_hole) ++*n_hole;
                 const float len = chord_hole(p.x, p.y, p.z, q.x, q.y, q.z, ha.x, ha.y, ha.z, ha.w, hbv.x);
+                if (len == 0.0f) continue;
+                if (n_cone) ++*n_cone;
+                const float4 c4 = *csp;
+                const ConeSelf cs{c4.x, c4.y, c4.z, c4.w};
+                int f = cone_filter(cs, p, ha.x, hbv.w, ha.w, hbv.z);
+                if (f < 0) f = cone_hole_exact(cs, p, ha.x, hbv.w, ha.w, hbv.z) ? 1 : 0;
+                if (!f) continue;
                 in_holes += len;
                 att += hbv.y * len;
                 if (RECORD && len > 0.0f) {
@@ -367,7 +379,7 @@ __device__ __forceinline__ float trace_ray(const PEParams& P, const DevGeometry&
     // Other crystals among the candidates, each in its own frame (:687-725).
     const int nwc = (L.n_c + 31) >> 5;
     for (int wd = 0; wd < nwc; ++wd) {
-        unsigned bits = mask_c[wd] & L.pass_c[wd];
+        unsigned bits = L.pass_c[wd];
         while (bits) {
             const int b = __ffs(bits) - 1;
             bits &= bits - 1;
@@ -384,6 +396,13 @@ __device__ __forceinline__ float trace_ray(const PEParams& P, const DevGeometry&
             const float zDa = (q.x - kp.x) * kr.y + (q.z - kp.z) * kr.x;
             const Box3 kb{-0.5f * ks.x, -0.5f * ks.y, -0.5f * ks.z, 0.5f * ks.x, 0.5f * ks.y, 0.5f * ks.z};
             const float len = chord_through(xIa, yIa, zIa, xDa, yDa, zDa, kb);
+            if (len == 0.0f) continue;
+            if (n_cone) ++*n_cone;
+            const float4 c4 = *csp;
+            const ConeSelf cs{c4.x, c4.y, c4.z, c4.w};
+            int f = cone_filter(cs, p, kp.x, kp.y, kp.z, 0.5f * ks.w);
+            if (f < 0) f = cone_crystal_exact(cs, p, kp.x, kp.y, kp.z, ks.w) ? 1 : 0;
+            if (!f) continue;
             att += len * kp.w;
             if (RECORD && len > 0.0f) {
                 if (rec_c < kRecCrystals) rec[3 + kRecHoles + rec_c] = S.c_id[k];
@@ -605,6 +624,7 @@ __device__ __forceinline__ void pe_tile(const PEParams& P, const DevGeometry& G,
         unsigned long long cnt_rays = 0, cnt_cry = 0, cnt_hole = 0, cnt_cone = 0;
         unsigned long long* pc_cry = P.counters ? &cnt_cry : nullptr;
         unsigned long long* pc_hole = P.counters ? &cnt_hole : nullptr;
+        unsigned long long* pc_cone = P.counters ? &cnt_cone : nullptr;
         // Entries of fewer than 32 rays go two voxels to a warp pass (P.pair):
         // the lanes of voxel 0 and voxel 1 are summed apart.
         const int VP = RECORD ? 1 : P.pair;
@@ -680,46 +700,14 @@ __device__ __forceinline__ void pe_tile(const PEParams& P, const DevGeometry& G,
                 const int n_pts = VP * P.n_sv;
                 for (int s0 = 0; s0 < n_pts; s0 += P.group) {
                     const int gn = min(P.group, n_pts - s0);
-                    // Candidate masks for points s0 .. s0+gn-1 (cone test on the lists).
-                    for (int j = 0; j < gn; ++j) {
-                        const int u = (VP == 1) ? 0 : (s0 + j) / P.n_sv;
-                        const Vec3 p = u == 0 ? subpoint_of(P, ix, iy, iz, s0 + j)
-                                              : subpoint_of(P, jx, jy, jz, s0 + j - P.n_sv);
+                    // The cone (ConeSelf) of each sub-point of the group, for the
+                    // cone tests trace_ray takes on the candidates a ray crosses.
+                    if (lane < gn) {
+                        const int u = (VP == 1) ? 0 : (s0 + lane) / P.n_sv;
+                        const Vec3 p = u == 0 ? subpoint_of(P, ix, iy, iz, s0 + lane)
+                                              : subpoint_of(P, jx, jy, jz, s0 + lane - P.n_sv);
                         const ConeSelf cs = cone_self(D, p);
-                        const Bundle bp = make_bundle(Box3{p.x, p.y, p.z, p.x, p.y, p.z}, D.world);
-                        for (int i0 = 0; i0 < lc; i0 += 32) {
-                            const int i = i0 + lane;
-                            bool pass = false;
-                            if (i < lc) {
-                                const int k = L.list_c[i];
-                                if (bundle_hit(bp, box_of(S.c_lo[k], S.c_hi[k]))) {
-                                    const float4 kp = S.c_pos[k];
-                                    const float crit = S.c_size[k].w;
-                                    int f = cone_filter(cs, p, kp.x, kp.y, kp.z, 0.5f * crit);
-                                    if (f < 0) f = cone_crystal_exact(cs, p, kp.x, kp.y, kp.z, crit) ? 1 : 0;
-                                    pass = f > 0;
-                                    if (P.counters) ++cnt_cone;
-                                }
-                            }
-                            const unsigned bal = __ballot_sync(0xffffffffu, pass);
-                            if (lane == 0) L.mask_c[j][i0 >> 5] = bal;
-                        }
-                        for (int i0 = 0; i0 < lh; i0 += 32) {
-                            const int i = i0 + lane;
-                            bool pass = false;
-                            if (i < lh) {
-                                const int k = L.list_h[i];
-                                const float4 ha = S.h_a[k], hb = S.h_b[k];
-                                if (bundle_hit(bp, hole_box(ha, hb))) {
-                                    int f = cone_filter(cs, p, ha.x, hb.w, ha.w, hb.z);
-                                    if (f < 0) f = cone_hole_exact(cs, p, ha.x, hb.w, ha.w, hb.z) ? 1 : 0;
-                                    pass = f > 0;
-                                    if (P.counters) ++cnt_cone;
-                                }
-                            }
-                            const unsigned bal = __ballot_sync(0xffffffffu, pass);
-                            if (lane == 0) L.mask_h[j][i0 >> 5] = bal;
-                        }
+                        L.cs[lane] = make_float4(cs.ux, cs.uy, cs.uz, cs.crit_self);
                     }
                     __syncwarp();
                     // Rays of the group, ordered (sub-cell column, sub-point, depth
@@ -762,15 +750,12 @@ __device__ __forceinline__ void pe_tile(const PEParams& P, const DevGeometry& G,
                             bz2 = fmaxf(bz2, __shfl_xor_sync(0xffffffffu, bz2, o));
                         }
                         const Bundle bq = make_bundle(Avox, Box3{bx1, by1, bz1, bx2, by2, bz2});
-                        // Narrow the group's candidates (any sub-point's mask) to
-                        // those the pass can reach; a candidate dropped here is one
-                        // that no ray of the pass can reach, i.e. one trace_ray would
-                        // skip by its own window test.
+                        // Narrow the voxel's candidates to those the pass can reach; a
+                        // candidate dropped here is one that no ray of the pass can
+                        // reach, i.e. one trace_ray would skip by its own window test.
                         for (int w = 0; w < nwc; ++w) {
-                            unsigned u = 0u;
-                            for (int jj = 0; jj < gn; ++jj) u |= L.mask_c[jj][w];
                             bool pass = false;
-                            if ((u >> lane) & 1u) {
+                            if ((w << 5) + lane < lc) {
                                 const int k = L.list_c[(w << 5) + lane];
                                 pass = bundle_hit(bq, box_of(S.c_lo[k], S.c_hi[k]));
                             }
@@ -778,10 +763,8 @@ __device__ __forceinline__ void pe_tile(const PEParams& P, const DevGeometry& G,
                             if (lane == 0) L.pass_c[w] = bal;
                         }
                         for (int w = 0; w < nwh; ++w) {
-                            unsigned u = 0u;
-                            for (int jj = 0; jj < gn; ++jj) u |= L.mask_h[jj][w];
                             bool pass = false;
-                            if ((u >> lane) & 1u) {
+                            if ((w << 5) + lane < lh) {
                                 const int k = L.list_h[(w << 5) + lane];
                                 pass = bundle_hit(bq, hole_box(S.h_a[k], S.h_b[k]));
                             }
@@ -802,8 +785,8 @@ __device__ __forceinline__ void pe_tile(const PEParams& P, const DevGeometry& G,
                                 rec = P.rec_out + ((long long)rec_slot * P.n_sv * P.n_sc + (long long)(s0 + j) * P.n_sc + c) *
                                                       kRecWords;
                             }
-                            const float v = trace_ray<RECORD>(P, G, S, L, L.mask_c[j], L.mask_h[j], D, p, ps, cell,
-                                                              rec, P.status, pc_cry, pc_hole);
+                            const float v = trace_ray<RECORD>(P, G, S, L, &L.cs[j], D, p, ps, cell, rec, P.status,
+                                                              pc_cry, pc_hole, pc_cone);
                             if (P.counters) ++cnt_rays;
                             // Kahan summation of the lane's rays.
                             const float y = v - comp;
