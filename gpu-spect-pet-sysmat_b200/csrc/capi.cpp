@@ -51,11 +51,6 @@ int context_collect_status(sm_context* ctx, cudaStream_t stream) {
     if (st != 0) {
         SM_CUDA(cudaMemsetAsync(ctx->d_status, 0, sizeof(int), stream));
         SM_CUDA(cudaStreamSynchronize(stream));
-        if (st & kStatusSupersetOverflow)
-            return fail(SM_ERR_CAPACITY,
-                        "a tile's candidate set exceeded %d crystals or %d holes; use smaller tile_voxels", kSupC, kSupH);
-        if (st & kStatusListOverflow)
-            return fail(SM_ERR_CAPACITY, "a voxel's candidate list exceeded %d crystals or %d holes", kListC, kListH);
         if (st & kStatusRecordOverflow)
             return fail(SM_ERR_CAPACITY, "a ray hit more than %d holes or %d crystals (hit record capacity)", kRecHoles,
                         kRecCrystals);

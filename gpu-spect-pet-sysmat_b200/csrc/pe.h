@@ -11,22 +11,21 @@ namespace smb {
 
 constexpr int kPeWarps = 8;            // warps per CTA = crystals per tile
 constexpr int kPeThreads = 32 * kPeWarps;
-constexpr int kSupC = 1024;            // tile superset capacity, crystals
+constexpr int kSupC = 1024;            // tile superset capacity, crystals (beyond: the tile's voxels use the tables)
 constexpr int kSupH = 384;             // tile superset capacity, holes
 constexpr int kMaxGroup = 8;           // voxel sub-points whose candidate masks are live at once
 constexpr int kMaxTileVoxels = 128;    // voxels per brick
-constexpr int kListC = 512;            // per-voxel candidate list capacity, crystals
+constexpr int kListC = 512;            // per-voxel candidate list capacity, crystals (beyond: the voxel uses the tables)
 constexpr int kListH = 128;            // per-voxel candidate list capacity, holes
 constexpr int kMaxSubcellsPerAxis = 64;
 constexpr int kRecHoles = 16;          // hit-record capacity per ray
 constexpr int kRecCrystals = 40;
 constexpr int kRecWords = 3 + kRecHoles + kRecCrystals;
 
-// Bits of the device status word.
+// Bits of the device status word.  (Candidate sets larger than the shared-memory
+// lists are not an error: those voxels are traced through the geometry tables.)
 enum : int {
-    kStatusSupersetOverflow = 1,
     kStatusRecordOverflow = 2,
-    kStatusListOverflow = 4,
 };
 
 struct PEParams {

@@ -56,6 +56,7 @@ constexpr int kLWC = kListC / 32;
 constexpr int kLWH = kListH / 32;
 constexpr float kMargin = 0.01f;     // mm added around every culling box
 constexpr float kConeMargin = 1e-5f; // float-filter band around the cone threshold
+constexpr int kPassSlots = 4;        // warp passes per group whose candidate masks are kept
 
 struct WarpLists {
     unsigned short list_c[kListC];    // staged-set indices of the voxel's candidate crystals
@@ -63,8 +64,11 @@ struct WarpLists {
     int n_c, n_h;
     int plate_begin[kMaxPlates + 1];  // list_h index where each plate's holes start
     float4 cs[kMaxGroup];             // per sub-point of the group: the detecting crystal's cone (ConeSelf)
-    unsigned pass_c[kLWC];            // per warp pass: candidates the pass's bundle of rays can reach
-    unsigned pass_h[kLWH];
+    // Per warp pass: the candidates the pass's bundle of rays can reach.  Slot
+    // i holds pass i of a group; full groups of one voxel trace the same
+    // sub-cells in the same passes, so later groups reuse the first one's.
+    unsigned pass_c[kPassSlots][kLWC];
+    unsigned pass_h[kPassSlots][kLWH];
 };
 
 struct __align__(16) PeSmem {
@@ -81,6 +85,7 @@ struct __align__(16) PeSmem {
     Box3 d_box[kPeWarps];    // inflated AABB of the tile's crystals
     int warp_cnt[kPeWarps];
     int n_c, n_h;
+    int overflow;            // the tile's candidates exceed the staged capacity: every voxel goes through the tables
     WarpLists wl[kPeWarps];
     float out[kPeWarps][kMaxTileVoxels];
 };
@@ -284,140 +289,10 @@ __device__ __noinline__ float self_path_exact(Vec3 ps, Vec3 qs, Box3 crystal, Bo
     return l1 - l2;
 }
 
-// Sub-cell centre in the detecting crystal's frame (xDs, yDs, zDs) and in the
-// world (q), as the reference computes them (PESysMatGen.cu:606-616).
-struct SubCell {
-    float xDs, yDs, zDs;
-    Vec3 q;
-};
-
-__device__ __forceinline__ SubCell sub_cell(const Detecting& D, const PeSmem& S, int sx, int sy, int sz) {
-    SubCell c;
-    c.xDs = -D.w / 2.0f + S.frac[0][sx] * D.w;
-    c.zDs = -D.h / 2.0f + S.frac[2][sz] * D.h;
-    c.yDs = -D.t / 2.0f + S.frac[1][sy] * D.t;
-    c.q.x = D.cx + (c.xDs * D.cp - c.zDs * D.sp);
-    c.q.z = D.cz + (c.xDs * D.sp + c.zDs * D.cp);
-    c.q.y = D.cy + c.yDs;
-    return c;
-}
-
-// One ray: sub-point p (world) and ps (detecting crystal frame), sub-cell
-// `cell`.  L.pass_c / L.pass_h: the candidates the warp pass's bundle of rays
-// can reach (a superset of those this ray can reach).  The reference counts a
-// crystal or hole only when it is among the sub-point's cone candidates
-// (PESysMatGen.cu:506-589); a candidate the ray does not cross adds nothing
-// either way, so the cone test (`csp`: the sub-point's ConeSelf) is taken only
-// for candidates with a nonzero chord.  Returns the contribution; in RECORD
-// mode also the hit record.
-template <bool RECORD>
-__device__ __forceinline__ float trace_ray(const PEParams& P, const DevGeometry& G, const PeSmem& S,
-                                           const WarpLists& L, const float4* csp, const Detecting& D, const Vec3& p,
-                                           const Vec3& ps, const SubCell& cell, int* rec, int* status,
-                                           unsigned long long* n_cry, unsigned long long* n_hole,
-                                           unsigned long long* n_cone) {
-    const float xDs = cell.xDs, yDs = cell.yDs, zDs = cell.zDs;
-    const Vec3 q = cell.q;
-
-    RaySeg seg;
-    seg.p = p;
-    seg.q = q;
-    seg.ordered = p.y < q.y;
-    const float dy = q.y - p.y;
-    seg.inv_dy = __fdividef(1.0f, dy);
-
-    unsigned plate_miss = 0u;
-    for (int m = 0; m < G.n_plates; ++m)
-        if (!plate_traversed(p, q, seg.inv_dy, G.plate[m])) plate_miss |= 1u << m;
-    if (!RECORD && plate_miss) return 0.0f;   // exp(-(1e5 + ...)) == 0
-
-    const float dxw = q.x - p.x, dzw = q.z - p.z;
-    const float dsq = fmaf(dy, dy, fmaf(dxw, dxw, dzw * dzw));
-    const float inv_r = rsqrtf(dsq);
-    const float r = dsq * inv_r;
-
-    int rec_h = 0, rec_c = 0;
-    float att = 0.0f;
-    // Plates: holes among the candidates, tungsten for the rest of T / cos(theta)
-    // (PESysMatGen.cu:661-685).
-    for (int m = 0; m < G.n_plates; ++m) {
-        float in_holes = 0.0f;
-        const int hb = L.plate_begin[m], he = L.plate_begin[m + 1];
-        for (int wd = hb >> 5; wd <= ((he - 1) >> 5) && he > hb; ++wd) {
-            unsigned bits = L.pass_h[wd];
-            const int lo = hb - (wd << 5), hi = he - (wd << 5);
-            if (lo > 0) bits &= ~0u << lo;
-            if (hi < 32) bits &= (1u << hi) - 1u;
-            while (bits) {
-                const int b = __ffs(bits) - 1;
-                bits &= bits - 1;
-                const int k = L.list_h[(wd << 5) + b];
-                const float4 ha = S.h_a[k], hbv = S.h_b[k];
-                if (!ray_may_hit(seg, hole_box(ha, hbv))) continue;
-                if (n_hole) ++*n_hole;
-                const float len = chord_hole(p.x, p.y, p.z, q.x, q.y, q.z, ha.x, ha.y, ha.z, ha.w, hbv.x);
-                if (len == 0.0f) continue;
-                if (n_cone) ++*n_cone;
-                const float4 c4 = *csp;
-                const ConeSelf cs{c4.x, c4.y, c4.z, c4.w};
-                int f = cone_filter(cs, p, ha.x, hbv.w, ha.w, hbv.z);
-                if (f < 0) f = cone_hole_exact(cs, p, ha.x, hbv.w, ha.w, hbv.z) ? 1 : 0;
-                if (!f) continue;
-                in_holes += len;
-                att += hbv.y * len;
-                if (RECORD && len > 0.0f) {
-                    if (rec_h < kRecHoles) rec[2 + rec_h] = S.h_id[k];
-                    else atomicOr(status, kStatusRecordOverflow);
-                    ++rec_h;
-                }
-            }
-        }
-        const PlateBox& pb = G.plate[m];
-        const float through = pb.thickness * r * seg.inv_dy;   // T / cos(theta)
-        if ((through - in_holes) >= 0.00001f) att += pb.mu_total * (through - in_holes);
-    }
-    // Other crystals among the candidates, each in its own frame (:687-725).
-    const int nwc = (L.n_c + 31) >> 5;
-    for (int wd = 0; wd < nwc; ++wd) {
-        unsigned bits = L.pass_c[wd];
-        while (bits) {
-            const int b = __ffs(bits) - 1;
-            bits &= bits - 1;
-            const int k = L.list_c[(wd << 5) + b];
-            if (!ray_may_hit(seg, box_of(S.c_lo[k], S.c_hi[k]))) continue;
-            if (n_cry) ++*n_cry;
-            const float4 kp = S.c_pos[k], ks = S.c_size[k];
-            const float2 kr = S.c_rot[k];
-            const float xIa = (p.x - kp.x) * kr.x - (p.z - kp.z) * kr.y;
-            const float yIa = p.y - kp.y;
-            const float zIa = (p.x - kp.x) * kr.y + (p.z - kp.z) * kr.x;
-            const float xDa = (q.x - kp.x) * kr.x - (q.z - kp.z) * kr.y;
-            const float yDa = q.y - kp.y;
-            const float zDa = (q.x - kp.x) * kr.y + (q.z - kp.z) * kr.x;
-            const Box3 kb{-0.5f * ks.x, -0.5f * ks.y, -0.5f * ks.z, 0.5f * ks.x, 0.5f * ks.y, 0.5f * ks.z};
-            const float len = chord_through(xIa, yIa, zIa, xDa, yDa, zDa, kb);
-            if (len == 0.0f) continue;
-            if (n_cone) ++*n_cone;
-            const float4 c4 = *csp;
-            const ConeSelf cs{c4.x, c4.y, c4.z, c4.w};
-            int f = cone_filter(cs, p, kp.x, kp.y, kp.z, 0.5f * ks.w);
-            if (f < 0) f = cone_crystal_exact(cs, p, kp.x, kp.y, kp.z, ks.w) ? 1 : 0;
-            if (!f) continue;
-            att += len * kp.w;
-            if (RECORD && len > 0.0f) {
-                if (rec_c < kRecCrystals) rec[3 + kRecHoles + rec_c] = S.c_id[k];
-                else atomicOr(status, kStatusRecordOverflow);
-                ++rec_c;
-            }
-        }
-    }
-    if (RECORD) {
-        rec[0] = (int)plate_miss;
-        rec[1] = rec_h < kRecHoles ? rec_h : kRecHoles;
-        rec[2 + kRecHoles] = rec_c < kRecCrystals ? rec_c : kRecCrystals;
-        if (plate_miss) return 0.0f;
-    }
-
+// Contribution of one ray once its attenuation outside the detecting crystal
+// is known: the path inside the detecting crystal, absorption and solid angle.
+__device__ __forceinline__ float ray_value(const Detecting& D, const Vec3& ps, float xDs, float yDs, float zDs,
+                                           float att, float r, float inv_r, float dxw, float dy, float dzw) {
     // Path inside the detecting crystal before the sub-cell and the absorption
     // chord (PESysMatGen.cu:727-759), as values: for the line from ps through
     // the sub-cell centre qs (direction u), the sub-cell entry lies at
@@ -459,15 +334,270 @@ __device__ __forceinline__ float trace_ray(const PEParams& P, const DevGeometry&
     return eff * sa * absorb;
 }
 
+// Sub-cell centre in the detecting crystal's frame (xDs, yDs, zDs) and in the
+// world (q), as the reference computes them (PESysMatGen.cu:606-616).
+struct SubCell {
+    float xDs, yDs, zDs;
+    Vec3 q;
+};
+
+__device__ __forceinline__ SubCell sub_cell(const Detecting& D, const PeSmem& S, int sx, int sy, int sz) {
+    SubCell c;
+    c.xDs = -D.w / 2.0f + S.frac[0][sx] * D.w;
+    c.zDs = -D.h / 2.0f + S.frac[2][sz] * D.h;
+    c.yDs = -D.t / 2.0f + S.frac[1][sy] * D.t;
+    c.q.x = D.cx + (c.xDs * D.cp - c.zDs * D.sp);
+    c.q.z = D.cz + (c.xDs * D.sp + c.zDs * D.cp);
+    c.q.y = D.cy + c.yDs;
+    return c;
+}
+
+// One ray: sub-point p (world) and ps (detecting crystal frame), sub-cell
+// `cell`.  pass_c / pass_h: the candidates the warp pass's bundle of rays
+// can reach (a superset of those this ray can reach).  The reference counts a
+// crystal or hole only when it is among the sub-point's cone candidates
+// (PESysMatGen.cu:506-589); a candidate the ray does not cross adds nothing
+// either way, so the cone test (`csp`: the sub-point's ConeSelf) is taken only
+// for candidates with a nonzero chord.  Returns the contribution; in RECORD
+// mode also the hit record.
+template <bool RECORD>
+__device__ __forceinline__ float trace_ray(const PEParams& P, const DevGeometry& G, const PeSmem& S,
+                                           const WarpLists& L, const unsigned* pass_c, const unsigned* pass_h,
+                                           const float4* csp, const Detecting& D, const Vec3& p,
+                                           const Vec3& ps, const SubCell& cell, int* rec, int* status,
+                                           unsigned long long* n_cry, unsigned long long* n_hole,
+                                           unsigned long long* n_cone) {
+    const float xDs = cell.xDs, yDs = cell.yDs, zDs = cell.zDs;
+    const Vec3 q = cell.q;
+
+    RaySeg seg;
+    seg.p = p;
+    seg.q = q;
+    seg.ordered = p.y < q.y;
+    const float dy = q.y - p.y;
+    seg.inv_dy = __fdividef(1.0f, dy);
+
+    unsigned plate_miss = 0u;
+    for (int m = 0; m < G.n_plates; ++m)
+        if (!plate_traversed(p, q, seg.inv_dy, G.plate[m])) plate_miss |= 1u << m;
+    if (!RECORD && plate_miss) return 0.0f;   // exp(-(1e5 + ...)) == 0
+
+    const float dxw = q.x - p.x, dzw = q.z - p.z;
+    const float dsq = fmaf(dy, dy, fmaf(dxw, dxw, dzw * dzw));
+    const float inv_r = rsqrtf(dsq);
+    const float r = dsq * inv_r;
+
+    int rec_h = 0, rec_c = 0;
+    float att = 0.0f;
+    // Plates: holes among the candidates, tungsten for the rest of T / cos(theta)
+    // (PESysMatGen.cu:661-685).
+    for (int m = 0; m < G.n_plates; ++m) {
+        float in_holes = 0.0f;
+        const int hb = L.plate_begin[m], he = L.plate_begin[m + 1];
+        for (int wd = hb >> 5; wd <= ((he - 1) >> 5) && he > hb; ++wd) {
+            unsigned bits = pass_h[wd];
+            const int lo = hb - (wd << 5), hi = he - (wd << 5);
+            if (lo > 0) bits &= ~0u << lo;
+            if (hi < 32) bits &= (1u << hi) - 1u;
+            while (bits) {
+                const int b = __ffs(bits) - 1;
+                bits &= bits - 1;
+                const int k = L.list_h[(wd << 5) + b];
+                const float4 ha = S.h_a[k], hbv = S.h_b[k];
+                if (!ray_may_hit(seg, hole_box(ha, hbv))) continue;
+                if (n_hole) ++*n_hole;
+                const float len = chord_hole(p.x, p.y, p.z, q.x, q.y, q.z, ha.x, ha.y, ha.z, ha.w, hbv.x);
+                if (len == 0.0f) continue;
+                if (n_cone) ++*n_cone;
+                const float4 c4 = *csp;
+                const ConeSelf cs{c4.x, c4.y, c4.z, c4.w};
+                int f = cone_filter(cs, p, ha.x, hbv.w, ha.w, hbv.z);
+                if (f < 0) f = cone_hole_exact(cs, p, ha.x, hbv.w, ha.w, hbv.z) ? 1 : 0;
+                if (!f) continue;
+                in_holes += len;
+                att += hbv.y * len;
+                if (RECORD && len > 0.0f) {
+                    if (rec_h < kRecHoles) rec[2 + rec_h] = S.h_id[k];
+                    else atomicOr(status, kStatusRecordOverflow);
+                    ++rec_h;
+                }
+            }
+        }
+        const PlateBox& pb = G.plate[m];
+        const float through = pb.thickness * r * seg.inv_dy;   // T / cos(theta)
+        if ((through - in_holes) >= 0.00001f) att += pb.mu_total * (through - in_holes);
+    }
+    // Other crystals among the candidates, each in its own frame (:687-725).
+    const int nwc = (L.n_c + 31) >> 5;
+    for (int wd = 0; wd < nwc; ++wd) {
+        unsigned bits = pass_c[wd];
+        while (bits) {
+            const int b = __ffs(bits) - 1;
+            bits &= bits - 1;
+            const int k = L.list_c[(wd << 5) + b];
+            if (!ray_may_hit(seg, box_of(S.c_lo[k], S.c_hi[k]))) continue;
+            if (n_cry) ++*n_cry;
+            const float4 kp = S.c_pos[k], ks = S.c_size[k];
+            const float2 kr = S.c_rot[k];
+            const float xIa = (p.x - kp.x) * kr.x - (p.z - kp.z) * kr.y;
+            const float yIa = p.y - kp.y;
+            const float zIa = (p.x - kp.x) * kr.y + (p.z - kp.z) * kr.x;
+            const float xDa = (q.x - kp.x) * kr.x - (q.z - kp.z) * kr.y;
+            const float yDa = q.y - kp.y;
+            const float zDa = (q.x - kp.x) * kr.y + (q.z - kp.z) * kr.x;
+            const Box3 kb{-0.5f * ks.x, -0.5f * ks.y, -0.5f * ks.z, 0.5f * ks.x, 0.5f * ks.y, 0.5f * ks.z};
+            const float len = chord_through(xIa, yIa, zIa, xDa, yDa, zDa, kb);
+            if (len == 0.0f) continue;
+            if (n_cone) ++*n_cone;
+            const float4 c4 = *csp;
+            const ConeSelf cs{c4.x, c4.y, c4.z, c4.w};
+            int f = cone_filter(cs, p, kp.x, kp.y, kp.z, 0.5f * ks.w);
+            if (f < 0) f = cone_crystal_exact(cs, p, kp.x, kp.y, kp.z, ks.w) ? 1 : 0;
+            if (!f) continue;
+            att += len * kp.w;
+            if (RECORD && len > 0.0f) {
+                if (rec_c < kRecCrystals) rec[3 + kRecHoles + rec_c] = S.c_id[k];
+                else atomicOr(status, kStatusRecordOverflow);
+                ++rec_c;
+            }
+        }
+    }
+    if (RECORD) {
+        rec[0] = (int)plate_miss;
+        rec[1] = rec_h < kRecHoles ? rec_h : kRecHoles;
+        rec[2 + kRecHoles] = rec_c < kRecCrystals ? rec_c : kRecCrystals;
+        if (plate_miss) return 0.0f;
+    }
+
+    return ray_value(D, ps, xDs, yDs, zDs, att, r, inv_r, dxw, dy, dzw);
+}
+
+// One ray with its candidates read straight from the geometry tables: every
+// hole and every other crystal, in id order, under the same window test,
+// exact chord and cone test as trace_ray.  For voxels whose candidate sets do
+// not fit the shared-memory lists (dense hole grids, very large detectors):
+// the same decisions and values, without a list.
+template <bool RECORD>
+__device__ __forceinline__ float trace_ray_global(const DevGeometry& G, const Detecting& D, int d, const Vec3& p,
+                                                  const Vec3& ps, const ConeSelf& cs, const SubCell& cell, int* rec,
+                                                  int* status) {
+    const float xDs = cell.xDs, yDs = cell.yDs, zDs = cell.zDs;
+    const Vec3 q = cell.q;
+    RaySeg seg;
+    seg.p = p;
+    seg.q = q;
+    seg.ordered = p.y < q.y;
+    const float dy = q.y - p.y;
+    seg.inv_dy = __fdividef(1.0f, dy);
+    unsigned plate_miss = 0u;
+    for (int m = 0; m < G.n_plates; ++m)
+        if (!plate_traversed(p, q, seg.inv_dy, G.plate[m])) plate_miss |= 1u << m;
+    if (!RECORD && plate_miss) return 0.0f;
+    const float dxw = q.x - p.x, dzw = q.z - p.z;
+    const float dsq = fmaf(dy, dy, fmaf(dxw, dxw, dzw * dzw));
+    const float inv_r = rsqrtf(dsq);
+    const float r = dsq * inv_r;
+    int rec_h = 0, rec_c = 0;
+    float att = 0.0f;
+    for (int m = 0; m < G.n_plates; ++m) {
+        float in_holes = 0.0f;
+        const int hb = G.plate[m].hole_begin, he = (m + 1 < G.n_plates) ? G.plate[m + 1].hole_begin : G.n_holes;
+        for (int k = hb; k < he; ++k) {
+            const float4 ha = G.h.a[k], hbv = G.h.b[k];
+            if (!ray_may_hit(seg, hole_box(ha, hbv))) continue;
+            const float len = chord_hole(p.x, p.y, p.z, q.x, q.y, q.z, ha.x, ha.y, ha.z, ha.w, hbv.x);
+            if (len == 0.0f) continue;
+            int f = cone_filter(cs, p, ha.x, hbv.w, ha.w, hbv.z);
+            if (f < 0) f = cone_hole_exact(cs, p, ha.x, hbv.w, ha.w, hbv.z) ? 1 : 0;
+            if (!f) continue;
+            in_holes += len;
+            att += hbv.y * len;
+            if (RECORD && len > 0.0f) {
+                if (rec_h < kRecHoles) rec[2 + rec_h] = k;
+                else atomicOr(status, kStatusRecordOverflow);
+                ++rec_h;
+            }
+        }
+        const PlateBox& pb = G.plate[m];
+        const float through = pb.thickness * r * seg.inv_dy;
+        if ((through - in_holes) >= 0.00001f) att += pb.mu_total * (through - in_holes);
+    }
+    for (int k = 0; k < G.n_crystals; ++k) {
+        if (k == d) continue;
+        const float4 lo = G.c.lo[k], hi = G.c.hi[k];
+        if (!ray_may_hit(seg, Box3{lo.x - kMargin, lo.y - kMargin, lo.z - kMargin, hi.x + kMargin, hi.y + kMargin,
+                                   hi.z + kMargin}))
+            continue;
+        const float4 kp = G.c.pos[k], ks = G.c.size[k], kr = G.c.rot[k];
+        const float xIa = (p.x - kp.x) * kr.x - (p.z - kp.z) * kr.y;
+        const float yIa = p.y - kp.y;
+        const float zIa = (p.x - kp.x) * kr.y + (p.z - kp.z) * kr.x;
+        const float xDa = (q.x - kp.x) * kr.x - (q.z - kp.z) * kr.y;
+        const float yDa = q.y - kp.y;
+        const float zDa = (q.x - kp.x) * kr.y + (q.z - kp.z) * kr.x;
+        const Box3 kb{-0.5f * ks.x, -0.5f * ks.y, -0.5f * ks.z, 0.5f * ks.x, 0.5f * ks.y, 0.5f * ks.z};
+        const float len = chord_through(xIa, yIa, zIa, xDa, yDa, zDa, kb);
+        if (len == 0.0f) continue;
+        int f = cone_filter(cs, p, kp.x, kp.y, kp.z, 0.5f * ks.w);
+        if (f < 0) f = cone_crystal_exact(cs, p, kp.x, kp.y, kp.z, ks.w) ? 1 : 0;
+        if (!f) continue;
+        att += len * kp.w;
+        if (RECORD && len > 0.0f) {
+            if (rec_c < kRecCrystals) rec[3 + kRecHoles + rec_c] = k;
+            else atomicOr(status, kStatusRecordOverflow);
+            ++rec_c;
+        }
+    }
+    if (RECORD) {
+        rec[0] = (int)plate_miss;
+        rec[1] = rec_h < kRecHoles ? rec_h : kRecHoles;
+        rec[2 + kRecHoles] = rec_c < kRecCrystals ? rec_c : kRecCrystals;
+        if (plate_miss) return 0.0f;
+    }
+    return ray_value(D, ps, xDs, yDs, zDs, att, r, inv_r, dxw, dy, dzw);
+}
+
+// The warp's sum over every ray of voxel (ix, iy, iz) for detecting crystal d
+// through trace_ray_global (same value on every lane); taken only for voxels
+// whose candidates overflow the lists.
+template <bool RECORD>
+__device__ __forceinline__ float slow_voxel(const PEParams& P, const DevGeometry& G, const PeSmem& S, const Detecting& D,
+                                         int d, int ix, int iy, int iz, int rec_slot, int lane) {
+    float acc = 0.0f, comp = 0.0f;
+    const int n = P.n_sv * P.n_sc;
+    for (int e = lane; e < n; e += 32) {
+        const int s = fast_div(e, P.n_sc, P.inv_n_sc);
+        const int c = e - s * P.n_sc;                      // (sz * dX + sx) * dY + sy, the oracle's order
+        const int t = fast_div(c, P.dY, P.inv_dY);
+        const int sy = c - t * P.dY;
+        const int sz = fast_div(t, P.dX, P.inv_dX);
+        const int sx = t - sz * P.dX;
+        const Vec3 p = subpoint_of(P, ix, iy, iz, s);
+        const ConeSelf cs = cone_self(D, p);
+        Vec3 ps;
+        ps.x = (p.x - D.cx) * D.cm - (p.z - D.cz) * D.sm;
+        ps.y = p.y - D.cy;
+        ps.z = (p.x - D.cx) * D.sm + (p.z - D.cz) * D.cm;
+        const SubCell cell = sub_cell(D, S, sx, sy, sz);
+        int* rec = nullptr;
+        if (RECORD) rec = P.rec_out + ((long long)rec_slot * P.n_sv * P.n_sc + (long long)e) * kRecWords;
+        const float v = trace_ray_global<RECORD>(G, D, d, p, ps, cs, cell, rec, P.status);
+        const float y = v - comp;
+        const float tt = acc + y;
+        comp = (tt - acc) - y;
+        acc = tt;
+    }
+    float v = acc - comp;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
 // Ordered compaction of a warp-wide predicate into a list; returns the new count.
-__device__ __forceinline__ int warp_append(bool pass, int value, unsigned short* list, int count, int cap, int lane,
-                                           int* status) {
+// Entries beyond `cap` are counted but not stored.
+__device__ __forceinline__ int warp_append(bool pass, int value, unsigned short* list, int count, int cap, int lane) {
     const unsigned bal = __ballot_sync(0xffffffffu, pass);
     const int pos = count + __popc(bal & lanemask_lt());
-    if (pass) {
-        if (pos < cap) list[pos] = (unsigned short)value;
-        else atomicOr(status, kStatusListOverflow);
-    }
+    if (pass && pos < cap) list[pos] = (unsigned short)value;
     return count + __popc(bal);
 }
 
@@ -553,14 +683,13 @@ __device__ __forceinline__ void pe_tile(const PEParams& P, const DevGeometry& G,
                 S.c_lo[off] = make_float4(lo.x - kMargin, lo.y - kMargin, lo.z - kMargin, 0.0f);
                 S.c_hi[off] = make_float4(hi.x + kMargin, hi.y + kMargin, hi.z + kMargin, 0.0f);
                 S.c_id[off] = k;
-            } else {
-                atomicOr(P.status, kStatusSupersetOverflow);
             }
         }
         base += total;
         __syncthreads();
     }
     const int n_c = min(base, kSupC);
+    const bool over_c = base > kSupC;
     base = 0;
     for (int k0 = 0; k0 < G.n_holes; k0 += kPeThreads) {
         const int k = k0 + tid;
@@ -587,8 +716,6 @@ __device__ __forceinline__ void pe_tile(const PEParams& P, const DevGeometry& G,
                 S.h_a[off] = ha;
                 S.h_b[off] = hb;
                 S.h_id[off] = k;
-            } else {
-                atomicOr(P.status, kStatusSupersetOverflow);
             }
         }
         base += total;
@@ -598,6 +725,7 @@ __device__ __forceinline__ void pe_tile(const PEParams& P, const DevGeometry& G,
     if (tid == 0) {
         S.n_c = n_c;
         S.n_h = n_h;
+        S.overflow = over_c || base > kSupH;
     }
     __syncthreads();
 
@@ -661,21 +789,23 @@ __device__ __forceinline__ void pe_tile(const PEParams& P, const DevGeometry& G,
                     Avox = Box3{fminf(Avox.x1, B2.x1), fminf(Avox.y1, B2.y1), fminf(Avox.z1, B2.z1),
                                 fmaxf(Avox.x2, B2.x2), fmaxf(Avox.y2, B2.y2), fmaxf(Avox.z2, B2.z2)};
                 }
-                {
+                bool slow = S.overflow != 0;
+                if (!slow) {
                     const Bundle bv = make_bundle(Avox, D.world);
                     int cnt = 0;
                     for (int k0 = 0; k0 < n_c; k0 += 32) {
                         const int k = k0 + lane;
                         const bool pass = k < n_c && S.c_id[k] != d && bundle_hit(bv, box_of(S.c_lo[k], S.c_hi[k]));
-                        cnt = warp_append(pass, k, L.list_c, cnt, kListC, lane, P.status);
+                        cnt = warp_append(pass, k, L.list_c, cnt, kListC, lane);
                     }
-                    cnt = min(cnt, kListC);
                     int cnth = 0;
                     for (int k0 = 0; k0 < n_h; k0 += 32) {
                         const int k = k0 + lane;
                         const bool pass = k < n_h && bundle_hit(bv, hole_box(S.h_a[k], S.h_b[k]));
-                        cnth = warp_append(pass, k, L.list_h, cnth, kListH, lane, P.status);
+                        cnth = warp_append(pass, k, L.list_h, cnth, kListH, lane);
                     }
+                    slow = cnt > kListC || cnth > kListH;
+                    cnt = min(cnt, kListC);
                     cnth = min(cnth, kListH);
                     __syncwarp();
                     // First list index of each plate's holes (hole ids ascend with the plate).
@@ -693,6 +823,18 @@ __device__ __forceinline__ void pe_tile(const PEParams& P, const DevGeometry& G,
                         L.n_h = cnth;
                     }
                     __syncwarp();
+                }
+                if (slow) {
+                    // The candidates do not fit the shared-memory lists: the voxel
+                    // (pair) through the geometry tables, same decisions and values.
+                    const float w0 = valid0 ? slow_voxel<RECORD>(P, G, S, D, d, ix, iy, iz, rec_slot, lane) : 0.0f;
+                    const float w1 = valid1 ? slow_voxel<RECORD>(P, G, S, D, d, jx, jy, jz, rec_slot, lane) : 0.0f;
+                    if (lane == 0) {
+                        if (valid0) S.out[warp][vl] = w0 * P.inv_sv;
+                        if (valid1) S.out[warp][vl + 1] = w1 * P.inv_sv;
+                    }
+                    __syncwarp();
+                    continue;
                 }
                 const int lc = L.n_c, lh = L.n_h;
                 const int nwc = (lc + 31) >> 5, nwh = (lh + 31) >> 5;
@@ -718,7 +860,11 @@ __device__ __forceinline__ void pe_tile(const PEParams& P, const DevGeometry& G,
                     const int cb = gn * P.dY;                  // rays per sub-cell column
                     const float inv_cb = 1.0f / (float)cb;
                     const int nr = gn * P.n_sc;
+                    // Full groups of one voxel deal the same sub-cells to the same
+                    // passes, so the first group's pass masks serve the others.
+                    const bool keep = VP == 1 && gn == P.group && nr <= 32 * kPassSlots;
                     for (int q0 = 0; q0 < nr; q0 += 32) {
+                        const int slot = keep ? (q0 >> 5) : 0;
                         const int e = q0 + lane;
                         bool active = e < nr;
                         int j = 0, sx = 0, sy = 0, sz = 0, u = 0;
@@ -736,40 +882,42 @@ __device__ __forceinline__ void pe_tile(const PEParams& P, const DevGeometry& G,
                             }
                         }
                         const SubCell cell = sub_cell(D, S, sx, sy, sz);
-                        // The pass's bundle: from the voxel's sub-point box to the
-                        // box of its rays' sub-cell centres.
-                        float bx1 = active ? cell.q.x : 3.0e38f, bx2 = active ? cell.q.x : -3.0e38f;
-                        float by1 = active ? cell.q.y : 3.0e38f, by2 = active ? cell.q.y : -3.0e38f;
-                        float bz1 = active ? cell.q.z : 3.0e38f, bz2 = active ? cell.q.z : -3.0e38f;
-                        for (int o = 16; o > 0; o >>= 1) {
-                            bx1 = fminf(bx1, __shfl_xor_sync(0xffffffffu, bx1, o));
-                            bx2 = fmaxf(bx2, __shfl_xor_sync(0xffffffffu, bx2, o));
-                            by1 = fminf(by1, __shfl_xor_sync(0xffffffffu, by1, o));
-                            by2 = fmaxf(by2, __shfl_xor_sync(0xffffffffu, by2, o));
-                            bz1 = fminf(bz1, __shfl_xor_sync(0xffffffffu, bz1, o));
-                            bz2 = fmaxf(bz2, __shfl_xor_sync(0xffffffffu, bz2, o));
-                        }
-                        const Bundle bq = make_bundle(Avox, Box3{bx1, by1, bz1, bx2, by2, bz2});
-                        // Narrow the voxel's candidates to those the pass can reach; a
-                        // candidate dropped here is one that no ray of the pass can
-                        // reach, i.e. one trace_ray would skip by its own window test.
-                        for (int w = 0; w < nwc; ++w) {
-                            bool pass = false;
-                            if ((w << 5) + lane < lc) {
-                                const int k = L.list_c[(w << 5) + lane];
-                                pass = bundle_hit(bq, box_of(S.c_lo[k], S.c_hi[k]));
+                        if (!(keep && s0 > 0)) {
+                            // The pass's bundle: from the voxel's sub-point box to the
+                            // box of its rays' sub-cell centres.
+                            float bx1 = active ? cell.q.x : 3.0e38f, bx2 = active ? cell.q.x : -3.0e38f;
+                            float by1 = active ? cell.q.y : 3.0e38f, by2 = active ? cell.q.y : -3.0e38f;
+                            float bz1 = active ? cell.q.z : 3.0e38f, bz2 = active ? cell.q.z : -3.0e38f;
+                            for (int o = 16; o > 0; o >>= 1) {
+                                bx1 = fminf(bx1, __shfl_xor_sync(0xffffffffu, bx1, o));
+                                bx2 = fmaxf(bx2, __shfl_xor_sync(0xffffffffu, bx2, o));
+                                by1 = fminf(by1, __shfl_xor_sync(0xffffffffu, by1, o));
+                                by2 = fmaxf(by2, __shfl_xor_sync(0xffffffffu, by2, o));
+                                bz1 = fminf(bz1, __shfl_xor_sync(0xffffffffu, bz1, o));
+                                bz2 = fmaxf(bz2, __shfl_xor_sync(0xffffffffu, bz2, o));
                             }
-                            const unsigned bal = __ballot_sync(0xffffffffu, pass);
-                            if (lane == 0) L.pass_c[w] = bal;
-                        }
-                        for (int w = 0; w < nwh; ++w) {
-                            bool pass = false;
-                            if ((w << 5) + lane < lh) {
-                                const int k = L.list_h[(w << 5) + lane];
-                                pass = bundle_hit(bq, hole_box(S.h_a[k], S.h_b[k]));
+                            const Bundle bq = make_bundle(Avox, Box3{bx1, by1, bz1, bx2, by2, bz2});
+                            // Narrow the voxel's candidates to those the pass can reach; a
+                            // candidate dropped here is one that no ray of the pass can
+                            // reach, i.e. one trace_ray would skip by its own window test.
+                            for (int w = 0; w < nwc; ++w) {
+                                bool pass = false;
+                                if ((w << 5) + lane < lc) {
+                                    const int k = L.list_c[(w << 5) + lane];
+                                    pass = bundle_hit(bq, box_of(S.c_lo[k], S.c_hi[k]));
+                                }
+                                const unsigned bal = __ballot_sync(0xffffffffu, pass);
+                                if (lane == 0) L.pass_c[slot][w] = bal;
                             }
-                            const unsigned bal = __ballot_sync(0xffffffffu, pass);
-                            if (lane == 0) L.pass_h[w] = bal;
+                            for (int w = 0; w < nwh; ++w) {
+                                bool pass = false;
+                                if ((w << 5) + lane < lh) {
+                                    const int k = L.list_h[(w << 5) + lane];
+                                    pass = bundle_hit(bq, hole_box(S.h_a[k], S.h_b[k]));
+                                }
+                                const unsigned bal = __ballot_sync(0xffffffffu, pass);
+                                if (lane == 0) L.pass_h[slot][w] = bal;
+                            }
                         }
                         __syncwarp();
                         if (active) {
@@ -785,7 +933,8 @@ __device__ __forceinline__ void pe_tile(const PEParams& P, const DevGeometry& G,
                                 rec = P.rec_out + ((long long)rec_slot * P.n_sv * P.n_sc + (long long)(s0 + j) * P.n_sc + c) *
                                                       kRecWords;
                             }
-                            const float v = trace_ray<RECORD>(P, G, S, L, &L.cs[j], D, p, ps, cell, rec, P.status,
+                            const float v = trace_ray<RECORD>(P, G, S, L, L.pass_c[slot], L.pass_h[slot], &L.cs[j], D,
+                                                              p, ps, cell, rec, P.status,
                                                               pc_cry, pc_hole, pc_cone);
                             if (P.counters) ++cnt_rays;
                             // Kahan summation of the lane's rays.

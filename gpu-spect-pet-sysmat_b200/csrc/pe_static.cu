@@ -291,11 +291,6 @@ extern "C" int sm_pe_compute_static(const float* collimator, size_t n_collimator
     int st = 0;
     SM_CUDA(cudaMemcpyAsync(&st, base, sizeof(int), cudaMemcpyDeviceToHost, stream));
     SM_CUDA(cudaStreamSynchronize(stream));
-    if (st & kStatusSupersetOverflow)
-        return fail(SM_ERR_CAPACITY, "a tile's candidate set exceeded %d crystals or %d holes; use smaller tile_voxels",
-                    kSupC, kSupH);
-    if (st & kStatusListOverflow)
-        return fail(SM_ERR_CAPACITY, "a voxel's candidate list exceeded %d crystals or %d holes", kListC, kListH);
     if (st != 0) return fail(SM_ERR_CUDA, "device status 0x%x", st);
     return SM_OK;
 }
