@@ -467,6 +467,10 @@ def run_beam_metrics(block, stream, reps: int = 5):
     with torch.cuda.stream(stream):
         beams.beam_metrics(block, stream=stream)          # warm-up
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        # Keep the GPU busy (~20 ms) while the host enqueues the timed calls, so
+        # that host-side delays (e.g. the CPU baseline's worker threads still
+        # spinning) leave no gaps between the timed kernels.
+        torch.cuda._sleep(40_000_000)
         e0.record(stream)
         for _ in range(reps):
             m = beams.beam_metrics(block, stream=stream)

@@ -64,6 +64,8 @@ struct WarpLists {
     int n_c, n_h;
     int plate_begin[kMaxPlates + 1];  // list_h index where each plate's holes start
     float4 cs[kMaxGroup];             // per sub-point of the group: the detecting crystal's cone (ConeSelf)
+    float4 pt[kMaxGroup];             // ... the sub-point in the world
+    float4 pself[kMaxGroup];          // ... and in the detecting crystal's frame
     // Per warp pass: the candidates the pass's bundle of rays can reach.  Slot
     // i holds pass i of a group; full groups of one voxel trace the same
     // sub-cells in the same passes, so later groups reuse the first one's.
@@ -182,7 +184,8 @@ __device__ __forceinline__ int cone_filter(const ConeSelf& cs, const Vec3& p, fl
     float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
     float inv = rsqrtf(d2);
     float ex = fmaf(dx, inv, -cs.ux), ey = fmaf(dy, inv, -cs.uy), ez = fmaf(dz, inv, -cs.uz);
-    float lhs = sqrtf(fmaf(ex, ex, fmaf(ey, ey, ez * ez)));
+    const float e2 = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
+    const float lhs = e2 > 0.0f ? e2 * rsqrtf(e2) : 0.0f;   // within 1e-6 relative of sqrt(e2)
     float rhs = fmaf(crit_scaled, inv, cs.crit_self);
     float diff = lhs - rhs;
     if (diff < -kConeMargin) return 1;
@@ -439,12 +442,25 @@ __device__ __forceinline__ float trace_ray(const PEParams& P, const DevGeometry&
             if (n_cry) ++*n_cry;
             const float4 kp = S.c_pos[k], ks = S.c_size[k];
             const float2 kr = S.c_rot[k];
-            const float xIa = (p.x - kp.x) * kr.x - (p.z - kp.z) * kr.y;
             const float yIa = p.y - kp.y;
-            const float zIa = (p.x - kp.x) * kr.y + (p.z - kp.z) * kr.x;
-            const float xDa = (q.x - kp.x) * kr.x - (q.z - kp.z) * kr.y;
             const float yDa = q.y - kp.y;
-            const float zDa = (q.x - kp.x) * kr.y + (q.z - kp.z) * kr.x;
+            float xIa, zIa, xDa, zDa;
+            if (kr.x == 1.0f && kr.y == 0.0f) {
+                // Unrotated crystal: a * 1 - b * (+-0) and a * (+-0) + b * 1
+                // round to a and b exactly.  Only the sign of a zero result
+                // can differ, and chord_through never divides by a coordinate:
+                // it subtracts them from nonzero box bounds, compares them, and
+                // divides only by differences of at least 0.001.
+                xIa = p.x - kp.x;
+                zIa = p.z - kp.z;
+                xDa = q.x - kp.x;
+                zDa = q.z - kp.z;
+            } else {
+                xIa = (p.x - kp.x) * kr.x - (p.z - kp.z) * kr.y;
+                zIa = (p.x - kp.x) * kr.y + (p.z - kp.z) * kr.x;
+                xDa = (q.x - kp.x) * kr.x - (q.z - kp.z) * kr.y;
+                zDa = (q.x - kp.x) * kr.y + (q.z - kp.z) * kr.x;
+            }
             const Box3 kb{-0.5f * ks.x, -0.5f * ks.y, -0.5f * ks.z, 0.5f * ks.x, 0.5f * ks.y, 0.5f * ks.z};
             const float len = chord_through(xIa, yIa, zIa, xDa, yDa, zDa, kb);
             if (len == 0.0f) continue;
@@ -850,6 +866,9 @@ __device__ __forceinline__ void pe_tile(const PEParams& P, const DevGeometry& G,
                                               : subpoint_of(P, jx, jy, jz, s0 + lane - P.n_sv);
                         const ConeSelf cs = cone_self(D, p);
                         L.cs[lane] = make_float4(cs.ux, cs.uy, cs.uz, cs.crit_self);
+                        L.pt[lane] = make_float4(p.x, p.y, p.z, 0.0f);
+                        L.pself[lane] = make_float4((p.x - D.cx) * D.cm - (p.z - D.cz) * D.sm, p.y - D.cy,
+                                                    (p.x - D.cx) * D.sm + (p.z - D.cz) * D.cm, 0.0f);
                     }
                     __syncwarp();
                     // Rays of the group, ordered (sub-cell column, sub-point, depth
@@ -921,12 +940,9 @@ __device__ __forceinline__ void pe_tile(const PEParams& P, const DevGeometry& G,
                         }
                         __syncwarp();
                         if (active) {
-                            const Vec3 p = u == 0 ? subpoint_of(P, ix, iy, iz, s0 + j)
-                                                  : subpoint_of(P, jx, jy, jz, s0 + j - P.n_sv);
-                            Vec3 ps;
-                            ps.x = (p.x - D.cx) * D.cm - (p.z - D.cz) * D.sm;
-                            ps.y = p.y - D.cy;
-                            ps.z = (p.x - D.cx) * D.sm + (p.z - D.cz) * D.cm;
+                            const float4 p4 = L.pt[j], ps4 = L.pself[j];
+                            const Vec3 p{p4.x, p4.y, p4.z};
+                            const Vec3 ps{ps4.x, ps4.y, ps4.z};
                             int* rec = nullptr;
                             if (RECORD) {
                                 const int c = (sz * P.dX + sx) * P.dY + sy;   // the oracle's sub-cell order
