@@ -61,7 +61,10 @@ constexpr int kPassSlots = 4;        // warp passes per group whose candidate ma
 struct WarpLists {
     unsigned short list_c[kListC];    // staged-set indices of the voxel's candidate crystals
     unsigned short list_h[kListH];    // ... and holes (ascending ids)
+    unsigned short blist_c[kListC];   // staged-set indices the whole brick can reach for this warp's crystal
+    unsigned short blist_h[kListH];   // (per-voxel lists narrow from these when they fit)
     int n_c, n_h;
+    int nb_c, nb_h;
     int plate_begin[kMaxPlates + 1];  // list_h index where each plate's holes start
     float4 cs[kMaxGroup];             // per sub-point of the group: the detecting crystal's cone (ConeSelf)
     float4 pt[kMaxGroup];             // ... the sub-point in the world
@@ -76,9 +79,8 @@ struct WarpLists {
 struct __align__(16) PeSmem {
     float4 c_pos[kSupC];     // cx, cy, cz, mu_total
     float4 c_size[kSupC];    // w, t, h, crit
-    float4 c_lo[kSupC];      // inflated world AABB
-    float4 c_hi[kSupC];
-    float2 c_rot[kSupC];     // cos(-rot), sin(-rot)
+    float4 c_lo[kSupC];      // inflated world AABB (lower corner), cos(-rot)
+    float4 c_hi[kSupC];      // ... (upper corner), sin(-rot)
     int c_id[kSupC];
     float4 h_a[kSupH];       // x, y1, y2, z
     float4 h_b[kSupH];       // R, mu_total, crit, yc
@@ -438,10 +440,11 @@ __device__ __forceinline__ float trace_ray(const PEParams& P, const DevGeometry&
             const int b = __ffs(bits) - 1;
             bits &= bits - 1;
             const int k = L.list_c[(wd << 5) + b];
-            if (!ray_may_hit(seg, box_of(S.c_lo[k], S.c_hi[k]))) continue;
+            const float4 klo = S.c_lo[k], khi = S.c_hi[k];
+            if (!ray_may_hit(seg, box_of(klo, khi))) continue;
             if (n_cry) ++*n_cry;
             const float4 kp = S.c_pos[k], ks = S.c_size[k];
-            const float2 kr = S.c_rot[k];
+            const float2 kr = make_float2(klo.w, khi.w);
             const float yIa = p.y - kp.y;
             const float yDa = q.y - kp.y;
             float xIa, zIa, xDa, zDa;
@@ -695,9 +698,8 @@ __device__ __forceinline__ void pe_tile(const PEParams& P, const DevGeometry& G,
                 S.c_pos[off] = G.c.pos[k];
                 S.c_size[off] = G.c.size[k];
                 const float4 rr = G.c.rot[k];
-                S.c_rot[off] = make_float2(rr.x, rr.y);
-                S.c_lo[off] = make_float4(lo.x - kMargin, lo.y - kMargin, lo.z - kMargin, 0.0f);
-                S.c_hi[off] = make_float4(hi.x + kMargin, hi.y + kMargin, hi.z + kMargin, 0.0f);
+                S.c_lo[off] = make_float4(lo.x - kMargin, lo.y - kMargin, lo.z - kMargin, rr.x);
+                S.c_hi[off] = make_float4(hi.x + kMargin, hi.y + kMargin, hi.z + kMargin, rr.y);
                 S.c_id[off] = k;
             }
         }
@@ -765,6 +767,31 @@ __device__ __forceinline__ void pe_tile(const PEParams& P, const DevGeometry& G,
             D.hz = 0.5f * D.h / (float)P.dZ;
         }
         const bool absorbing = D.mu_t > 0.01f;   // PESysMatGen.cu:504, :598
+        // Candidates the whole brick can reach for this crystal (bundle from the
+        // brick's sub-point box A): the per-voxel lists narrow from these when
+        // they fit, instead of from the tile's staged set.
+        bool brick = false;
+        if (absorbing && !S.overflow) {
+            const Bundle bb = make_bundle(A, D.world);
+            int nb = 0;
+            for (int k0 = 0; k0 < n_c; k0 += 32) {
+                const int k = k0 + lane;
+                const bool pass = k < n_c && S.c_id[k] != d && bundle_hit(bb, box_of(S.c_lo[k], S.c_hi[k]));
+                nb = warp_append(pass, k, L.blist_c, nb, kListC, lane);
+            }
+            int nbh = 0;
+            for (int k0 = 0; k0 < n_h; k0 += 32) {
+                const int k = k0 + lane;
+                const bool pass = k < n_h && bundle_hit(bb, hole_box(S.h_a[k], S.h_b[k]));
+                nbh = warp_append(pass, k, L.blist_h, nbh, kListH, lane);
+            }
+            brick = nb <= kListC && nbh <= kListH;
+            if (lane == 0) {
+                L.nb_c = nb;
+                L.nb_h = nbh;
+            }
+            __syncwarp();
+        }
         unsigned long long cnt_rays = 0, cnt_cry = 0, cnt_hole = 0, cnt_cone = 0;
         unsigned long long* pc_cry = P.counters ? &cnt_cry : nullptr;
         unsigned long long* pc_hole = P.counters ? &cnt_hole : nullptr;
@@ -809,15 +836,27 @@ __device__ __forceinline__ void pe_tile(const PEParams& P, const DevGeometry& G,
                 if (!slow) {
                     const Bundle bv = make_bundle(Avox, D.world);
                     int cnt = 0;
-                    for (int k0 = 0; k0 < n_c; k0 += 32) {
-                        const int k = k0 + lane;
-                        const bool pass = k < n_c && S.c_id[k] != d && bundle_hit(bv, box_of(S.c_lo[k], S.c_hi[k]));
+                    const int src_c = brick ? L.nb_c : n_c;
+                    for (int i0 = 0; i0 < src_c; i0 += 32) {
+                        const int i = i0 + lane;
+                        int k = i;
+                        bool pass = false;
+                        if (i < src_c) {
+                            k = brick ? (int)L.blist_c[i] : i;
+                            pass = (brick || S.c_id[k] != d) && bundle_hit(bv, box_of(S.c_lo[k], S.c_hi[k]));
+                        }
                         cnt = warp_append(pass, k, L.list_c, cnt, kListC, lane);
                     }
                     int cnth = 0;
-                    for (int k0 = 0; k0 < n_h; k0 += 32) {
-                        const int k = k0 + lane;
-                        const bool pass = k < n_h && bundle_hit(bv, hole_box(S.h_a[k], S.h_b[k]));
+                    const int src_h = brick ? L.nb_h : n_h;
+                    for (int i0 = 0; i0 < src_h; i0 += 32) {
+                        const int i = i0 + lane;
+                        int k = i;
+                        bool pass = false;
+                        if (i < src_h) {
+                            k = brick ? (int)L.blist_h[i] : i;
+                            pass = bundle_hit(bv, hole_box(S.h_a[k], S.h_b[k]));
+                        }
                         cnth = warp_append(pass, k, L.list_h, cnth, kListH, lane);
                     }
                     slow = cnt > kListC || cnth > kListH;
@@ -901,7 +940,18 @@ __device__ __forceinline__ void pe_tile(const PEParams& P, const DevGeometry& G,
                             }
                         }
                         const SubCell cell = sub_cell(D, S, sx, sy, sz);
-                        if (!(keep && s0 > 0)) {
+                        if (nr <= 32) {
+                            // One pass holds every ray of the group: its bundle is the
+                            // voxel's own, which the list was built from.
+                            if (lane < nwc) {
+                                const int n_in = lc - (lane << 5);
+                                L.pass_c[slot][lane] = n_in >= 32 ? 0xffffffffu : ((1u << n_in) - 1u);
+                            }
+                            if (lane < nwh) {
+                                const int n_in = lh - (lane << 5);
+                                L.pass_h[slot][lane] = n_in >= 32 ? 0xffffffffu : ((1u << n_in) - 1u);
+                            }
+                        } else if (!(keep && s0 > 0)) {
                             // The pass's bundle: from the voxel's sub-point box to the
                             // box of its rays' sub-cell centres.
                             float bx1 = active ? cell.q.x : 3.0e38f, bx2 = active ? cell.q.x : -3.0e38f;
