@@ -12,9 +12,9 @@
 //
 // Work decomposition (one CTA per tile = 8 crystals x one voxel brick):
 //  1. Tile cull: the CTA tests every crystal and hole against the bundle of
-//     segments from the brick's sub-point box to each of its 8 crystals
-//     (window_hit, conservative) and stages the survivors, ordered by id, in
-//     shared memory.
+//     segments from the brick's sub-point box to the union of its 8 crystals,
+//     then to each crystal (division-free window test, conservative), and
+//     stages the survivors, ordered by id, in shared memory.
 //  2. Each warp owns one crystal and walks the brick's voxels.  Per voxel it
 //     narrows the staged set with the same window test for that voxel's
 //     sub-point box and compacts the survivors into a per-warp list.  The
@@ -671,6 +671,22 @@ __device__ __forceinline__ void pe_tile(const PEParams& P, const DevGeometry& G,
     }
     __syncthreads();
     const int n_d = min(kPeWarps, P.row1 - d0);
+    // The tile's crystals side by side: a candidate the bundle from A to their
+    // union box misses is missed by every crystal's own bundle.
+    Box3 U = S.d_box[0];
+    for (int j = 1; j < n_d; ++j) {
+        const Box3 b = S.d_box[j];
+        U = Box3{fminf(U.x1, b.x1), fminf(U.y1, b.y1), fminf(U.z1, b.z1), fmaxf(U.x2, b.x2), fmaxf(U.y2, b.y2),
+                 fmaxf(U.z2, b.z2)};
+    }
+    const Bundle bu = make_bundle(A, U);
+    auto tile_hit = [&](const Box3& K) {
+        if (!bundle_hit(bu, K)) return false;
+        if (n_d == 1) return true;
+        for (int j = 0; j < n_d; ++j)
+            if (bundle_hit(make_bundle(A, S.d_box[j]), K)) return true;
+        return false;
+    };
 
     int base = 0;
     for (int k0 = 0; k0 < G.n_crystals; k0 += kPeThreads) {
@@ -681,7 +697,7 @@ __device__ __forceinline__ void pe_tile(const PEParams& P, const DevGeometry& G,
             lo = G.c.lo[k];
             hi = G.c.hi[k];
             const Box3 K{lo.x - kMargin, lo.y - kMargin, lo.z - kMargin, hi.x + kMargin, hi.y + kMargin, hi.z + kMargin};
-            for (int j = 0; j < n_d && !pass; ++j) pass = window_hit(A, S.d_box[j], K);
+            pass = tile_hit(K);
         }
         const unsigned bal = __ballot_sync(0xffffffffu, pass);
         if (lane == 0) S.warp_cnt[warp] = __popc(bal);
@@ -717,7 +733,7 @@ __device__ __forceinline__ void pe_tile(const PEParams& P, const DevGeometry& G,
             ha = G.h.a[k];
             hb = G.h.b[k];
             const Box3 K = hole_box(ha, hb);
-            for (int j = 0; j < n_d && !pass; ++j) pass = window_hit(A, S.d_box[j], K);
+            pass = tile_hit(K);
         }
         const unsigned bal = __ballot_sync(0xffffffffu, pass);
         if (lane == 0) S.warp_cnt[warp] = __popc(bal);
