@@ -38,7 +38,7 @@ struct PEParams {
     float cos_a, sin_a;      // image rotation about z
     int dX, dY, dZ;          // crystal sub-cells
     int n_sc, n_sv, group;   // sub-cells per crystal, sub-points per voxel, sub-points per mask group
-    int pair;                // voxels per warp pass: 2 when a voxel has at most 16 rays, else 1
+    int pair;                // voxels per group of sub-points (1..8): > 1 when a voxel has at most 16 rays
     float inv_sv;
     // reciprocals for the division-free index decode (exact after one correction step)
     float inv_n_sc, inv_dY, inv_dX, inv_kx, inv_ky, inv_kxky, inv_dXdY;

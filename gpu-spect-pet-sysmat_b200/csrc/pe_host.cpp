@@ -44,10 +44,22 @@ void pe_plan(const HostGeometry& g, const int sv[3], const int sc[3], const int 
     P.n_sc = sc[0] * sc[1] * sc[2];
     P.n_sv = sv[0] * sv[1] * sv[2];
     P.group = group > 0 ? std::min(group, kMaxGroup) : pe_auto_group(P.dY);
-    // An entry of at most 16 rays fills half a warp: two voxels share each
-    // warp pass, as one group of both voxels' sub-points.
-    P.pair = (P.n_sv * P.n_sc <= 16 && 2 * P.n_sv <= kMaxGroup) ? 2 : 1;
-    if (P.pair == 2) P.group = 2 * P.n_sv;
+    // Entries of at most 16 rays: VP neighbouring voxels form one group of
+    // sub-points (VP * n_sv <= kMaxGroup), so that a warp pass traces one
+    // sub-cell column from all of them.  The kernel sums each lane's rays for
+    // one voxel, so the lane-to-point map must be the same in every pass: the
+    // group's rays fit one pass, or a sub-cell column's rays (cb) divide 32.
+    P.pair = 1;
+    if (P.n_sv * P.n_sc <= 16) {
+        for (int vp = 8; vp >= 2; vp >>= 1) {
+            const int g = vp * P.n_sv, cb = g * P.dY;
+            if (g <= kMaxGroup && (g * P.n_sc <= 32 || (cb <= 32 && 32 % cb == 0))) {
+                P.pair = vp;
+                break;
+            }
+        }
+    }
+    if (P.pair > 1) P.group = P.pair * P.n_sv;
     P.inv_sv = 1.0f / (float)P.n_sv;
     P.inv_n_sc = 1.0f / (float)P.n_sc;
     P.inv_dY = 1.0f / (float)P.dY;

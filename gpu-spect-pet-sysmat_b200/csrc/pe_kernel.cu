@@ -812,23 +812,32 @@ __device__ __forceinline__ void pe_tile(const PEParams& P, const DevGeometry& G,
         unsigned long long* pc_cry = P.counters ? &cnt_cry : nullptr;
         unsigned long long* pc_hole = P.counters ? &cnt_hole : nullptr;
         unsigned long long* pc_cone = P.counters ? &cnt_cone : nullptr;
-        // Entries of fewer than 32 rays go two voxels to a warp pass (P.pair):
-        // the lanes of voxel 0 and voxel 1 are summed apart.
+        // Entries of few rays go VP neighbouring voxels of the brick to a group
+        // (P.pair, up to 8): a pass then traces one sub-cell column from all of
+        // them, and the lanes of each voxel are summed apart.
         const int VP = RECORD ? 1 : P.pair;
         for (int vl = 0; vl < tv; vl += VP) {
-            const int ix = ix0 + vl % P.bx;
-            const int iy = iy0 + (vl / P.bx) % P.by;
-            const int iz = iz0 + vl / (P.bx * P.by);
-            const bool valid0 = ix < ix1 && iy < iy1 && iz < iz1;
-            int jx = 0, jy = 0, jz = 0;
-            bool valid1 = false;
-            if (VP == 2 && vl + 1 < tv) {
-                jx = ix0 + (vl + 1) % P.bx;
-                jy = iy0 + ((vl + 1) / P.bx) % P.by;
-                jz = iz0 + (vl + 1) / (P.bx * P.by);
-                valid1 = jx < ix1 && jy < iy1 && jz < iz1;
+            // voxel u of the group is brick voxel vl + u
+            auto vox_of = [&](int u, int& x, int& y, int& z) {
+                const int b = vl + u;
+                x = ix0 + b % P.bx;
+                y = iy0 + (b / P.bx) % P.by;
+                z = iz0 + b / (P.bx * P.by);
+            };
+            int ix, iy, iz;
+            vox_of(0, ix, iy, iz);
+            unsigned valid = 0u;
+            int lox = 1 << 30, loy = 1 << 30, loz = 1 << 30, hix = -1, hiy = -1, hiz = -1;
+            for (int u = 0; u < VP; ++u) {
+                int x, y, z;
+                vox_of(u, x, y, z);
+                if (vl + u < tv && x < ix1 && y < iy1 && z < iz1) {
+                    valid |= 1u << u;
+                    lox = min(lox, x); loy = min(loy, y); loz = min(loz, z);
+                    hix = max(hix, x); hiy = max(hiy, y); hiz = max(hiz, z);
+                }
             }
-            if (!valid0 && !valid1) continue;
+            if (!valid) continue;
             int rec_slot = -1;
             if (RECORD) {
                 const long long vox = ((long long)iz * P.ny + iy) * P.nx + ix;
@@ -840,14 +849,9 @@ __device__ __forceinline__ void pe_tile(const PEParams& P, const DevGeometry& G,
             int lane_vox = 0;
             if (absorbing) {
                 // Voxel-level candidate lists: staged crystals/holes the bundle from
-                // the sub-points of this voxel (or voxel pair) to the crystal can reach.
-                Box3 Avox = valid0 ? point_box_of(ix, iy, iz, ix + 1, iy + 1, iz + 1)
-                                   : point_box_of(jx, jy, jz, jx + 1, jy + 1, jz + 1);
-                if (valid0 && valid1) {
-                    const Box3 B2 = point_box_of(jx, jy, jz, jx + 1, jy + 1, jz + 1);
-                    Avox = Box3{fminf(Avox.x1, B2.x1), fminf(Avox.y1, B2.y1), fminf(Avox.z1, B2.z1),
-                                fmaxf(Avox.x2, B2.x2), fmaxf(Avox.y2, B2.y2), fmaxf(Avox.z2, B2.z2)};
-                }
+                // the sub-points of the group's voxels (the box of their voxel
+                // range) to the crystal can reach.
+                const Box3 Avox = point_box_of(lox, loy, loz, hix + 1, hiy + 1, hiz + 1);
                 bool slow = S.overflow != 0;
                 if (!slow) {
                     const Bundle bv = make_bundle(Avox, D.world);
@@ -896,20 +900,21 @@ __device__ __forceinline__ void pe_tile(const PEParams& P, const DevGeometry& G,
                     __syncwarp();
                 }
                 if (slow) {
-                    // The candidates do not fit the shared-memory lists: the voxel
-                    // (pair) through the geometry tables, same decisions and values.
-                    const float w0 = valid0 ? slow_voxel<RECORD>(P, G, S, D, d, ix, iy, iz, rec_slot, lane) : 0.0f;
-                    const float w1 = valid1 ? slow_voxel<RECORD>(P, G, S, D, d, jx, jy, jz, rec_slot, lane) : 0.0f;
-                    if (lane == 0) {
-                        if (valid0) S.out[warp][vl] = w0 * P.inv_sv;
-                        if (valid1) S.out[warp][vl + 1] = w1 * P.inv_sv;
+                    // The candidates do not fit the shared-memory lists: the group's
+                    // voxels through the geometry tables, same decisions and values.
+                    for (int u = 0; u < VP; ++u) {
+                        if (!((valid >> u) & 1u)) continue;
+                        int x, y, z;
+                        vox_of(u, x, y, z);
+                        const float w = slow_voxel<RECORD>(P, G, S, D, d, x, y, z, rec_slot, lane);
+                        if (lane == 0) S.out[warp][vl + u] = w * P.inv_sv;
                     }
                     __syncwarp();
                     continue;
                 }
                 const int lc = L.n_c, lh = L.n_h;
                 const int nwc = (lc + 31) >> 5, nwh = (lh + 31) >> 5;
-                // points of the pass(es): sub-points of voxel 0, then of voxel 1
+                // points of the group: the sub-points of voxel 0, then of voxel 1, ...
                 const int n_pts = VP * P.n_sv;
                 for (int s0 = 0; s0 < n_pts; s0 += P.group) {
                     const int gn = min(P.group, n_pts - s0);
@@ -917,8 +922,9 @@ __device__ __forceinline__ void pe_tile(const PEParams& P, const DevGeometry& G,
                     // cone tests trace_ray takes on the candidates a ray crosses.
                     if (lane < gn) {
                         const int u = (VP == 1) ? 0 : (s0 + lane) / P.n_sv;
-                        const Vec3 p = u == 0 ? subpoint_of(P, ix, iy, iz, s0 + lane)
-                                              : subpoint_of(P, jx, jy, jz, s0 + lane - P.n_sv);
+                        int x = ix, y = iy, z = iz;
+                        if (u > 0) vox_of(u, x, y, z);
+                        const Vec3 p = subpoint_of(P, x, y, z, s0 + lane - u * P.n_sv);
                         const ConeSelf cs = cone_self(D, p);
                         L.cs[lane] = make_float4(cs.ux, cs.uy, cs.uz, cs.crit_self);
                         L.pt[lane] = make_float4(p.x, p.y, p.z, 0.0f);
@@ -949,9 +955,9 @@ __device__ __forceinline__ void pe_tile(const PEParams& P, const DevGeometry& G,
                             sy = r - j * P.dY;
                             sz = fast_div(col, P.dX, P.inv_dX);
                             sx = col - sz * P.dX;
-                            if (VP == 2) {
+                            if (VP > 1) {
                                 u = (s0 + j) / P.n_sv;
-                                active = u == 0 ? valid0 : valid1;
+                                active = (valid >> u) & 1u;
                                 lane_vox = u;
                             }
                         }
@@ -1030,17 +1036,13 @@ __device__ __forceinline__ void pe_tile(const PEParams& P, const DevGeometry& G,
                     __syncwarp();
                 }
             }
-            float v = acc - comp;
-            float v1 = 0.0f;
-            if (VP == 2) {
-                v1 = lane_vox == 1 ? v : 0.0f;
-                v = lane_vox == 0 ? v : 0.0f;
-                for (int o = 16; o > 0; o >>= 1) v1 += __shfl_xor_sync(0xffffffffu, v1, o);
-            }
-            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-            if (lane == 0) {
-                if (valid0) S.out[warp][vl] = v * P.inv_sv;
-                if (valid1) S.out[warp][vl + 1] = v1 * P.inv_sv;
+            const float v = acc - comp;
+            for (int u = 0; u < VP; ++u) {
+                // a lane's rays all belong to one voxel of the group (pe_plan
+                // picks VP so that the lane-to-point map is the same every pass)
+                float w = lane_vox == u ? v : 0.0f;
+                for (int o = 16; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
+                if (lane == 0 && ((valid >> u) & 1u)) S.out[warp][vl + u] = w * P.inv_sv;
             }
         }
         if (P.counters) {

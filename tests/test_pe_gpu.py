@@ -151,9 +151,10 @@ def test_tiling_slabs_and_rows_do_not_change_results(ctx):
 
 
 def test_voxel_pairs_do_not_change_results(ctx):
-    """Entries of at most 16 rays (voxel centre x 2x4x2 sub-cells) go two voxels
-    to a warp pass; which neighbour a voxel is paired with (it depends on the
-    brick) changes no value, and a voxel alone in a pass gives the same."""
+    """Entries of at most 16 rays (voxel centre x 2x4x2 sub-cells) go up to 8
+    neighbouring voxels to a group of sub-points; which neighbours a voxel is
+    grouped with (it depends on the brick) changes no value, and a voxel alone
+    in its group gives the same."""
     p = configs.tiny(layers=3)
     g = sysmat_b200.Geometry(ctx, p)
     full = g.pe()
