@@ -40,10 +40,10 @@ sys.path.insert(0, os.path.join(ROOT, "gpu-spect-pet-sysmat_b200"))
 SLAB_Z = 4
 L2_FLUSH_BYTES = 256 << 20
 # DRAM traffic of one full pe_large slab launch (6400 x 16384 entries):
-# dram__bytes_read.sum 128.87 MB + dram__bytes_write.sum 589.75 MB from one
+# dram__bytes_read.sum 126.68 MB + dram__bytes_write.sum 579.35 MB from one
 # single-pass ncu capture of pe_trace_kernel on B200.  Algorithmic bytes of the
 # same launch: 4 B per entry of output, 419.4 MB, plus 0.64 MB of tables.
-PE_LARGE_SLAB_DRAM_BYTES = 718.62e6
+PE_LARGE_SLAB_DRAM_BYTES = 706.03e6
 PE_LARGE_SLAB_ALGORITHMIC_BYTES = 4 * 6400 * 16384 + 2 * 4 * 80000
 
 # FP32 operations per unit of work, counted from the tracer's source
