@@ -182,7 +182,8 @@ int sm_pe_autotune(sm_context* ctx, const sm_geometry* geo, const sm_pe_options*
                 if (rc == SM_OK) cudaEventElapsedTime(&ms, e0, e1);
                 if (rep > 0) t_best = std::min(t_best, (double)ms);   // the first run warms up
             }
-            // a brick whose timed tiles overflow a candidate list is not a candidate
+            // a launch that reports a device status bit is not a candidate (voxels whose
+            // candidates overflow the lists are traced through the tables: slower, not an error)
             int st = 0;
             if (rc == SM_OK) rc = check_cuda(cudaMemcpy(&st, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost), "status");
             if (rc == SM_OK && st != 0) {
