@@ -171,7 +171,8 @@ int sm_pe_record_hits(sm_context* ctx, const sm_geometry* geo, const sm_pe_optio
 
 /* Work counters: when enabled, each sm_pe_compute on the context counts rays
  * traced, exact crystal tests, exact hole tests and candidate cone tests
- * (costs a little time and synchronises the call). */
+ * (the cone test is taken on the candidates a ray crosses) (costs a little
+ * time and synchronises the call). */
 int sm_pe_set_counters(sm_context* ctx, int enable);
 int sm_pe_last_counters(sm_context* ctx, int64_t out[4]);
 
