@@ -94,6 +94,10 @@ struct __align__(16) PeSmem {
     float out[kPeWarps][kMaxTileVoxels];
 };
 
+// Two CTAs per SM (the kernel's launch bound): an SM holds 228 KB of shared
+// memory, of which each CTA also reserves 1 KB.
+static_assert(2 * (sizeof(PeSmem) + 1024) <= 228 * 1024, "PeSmem must leave room for two CTAs per SM");
+
 __device__ __forceinline__ unsigned lanemask_lt() {
     unsigned m;
     asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
